@@ -1,0 +1,124 @@
+/* mckl_b200.h -- C ABI of the B200 (sm_100a) implementation of MCKL's
+ * counter-based RNG, distribution and SMC hot path.
+ *
+ * Conventions (all entry points):
+ *   - `extern "C"`, plain pointers and sizes; returns an int status
+ *     (MCKL_B200_OK == 0, negative on error; mckl_b200_last_error() gives the
+ *     message).  No exception crosses this boundary.
+ *   - Array arguments named `*_dev` / documented as device pointers must be
+ *     addressable by the device: CUDA device memory, or page-locked host
+ *     memory (cudaHostAlloc / cudaHostRegister), which kernels then read and
+ *     write over the host link.  Engine states and scalar results live on the
+ *     host.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *     stream).  Work is enqueued on it; a call returns before the GPU finishes
+ *     unless its comment says it synchronizes.
+ *   - Engine state is updated on the host exactly as the reference's
+ *     CounterEngine would be after the same call sequence, so states stay
+ *     interchangeable with mckl::Philox4x32 / Threefry4x64 / ARS (and _64).
+ *
+ * Reference citations are to the MCKL source tree (zhouyan/MCKL).
+ */
+#ifndef MCKL_B200_H
+#define MCKL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MCKL_B200_OK 0
+#define MCKL_B200_ERR_ARG (-1)     /* invalid argument (size, kind, null pointer) */
+#define MCKL_B200_ERR_CUDA (-2)    /* a CUDA runtime call failed */
+#define MCKL_B200_ERR_NOMEM (-3)   /* device scratch could not be obtained */
+#define MCKL_B200_ERR_DEVICE (-4)  /* a kernel reported an error status */
+
+/* Engine kinds: the reference's engine aliases with 32- and 64-bit results. */
+#define MCKL_B200_PHILOX4X32 1      /* mckl::Philox4x32     random/philox.hpp:216    */
+#define MCKL_B200_PHILOX4X32_64 2   /* mckl::Philox4x32_64  random/philox.hpp:232    */
+#define MCKL_B200_THREEFRY4X64 3    /* mckl::Threefry4x64   random/threefry.hpp:271  */
+#define MCKL_B200_THREEFRY4X64_64 4 /* mckl::Threefry4x64_64 random/threefry.hpp:307 */
+#define MCKL_B200_ARS 5             /* mckl::ARS            random/aes.hpp:256       */
+#define MCKL_B200_ARS_64 6          /* mckl::ARS_64         random/aes.hpp:272       */
+
+/* State of one counter-based engine: mckl::CounterEngine<ResultType, Generator>
+ * (random/counter.hpp:61-288).  `ctr` is the counter of the last generated
+ * block in the reference's Counter layout (Counter<u32,4> = 2 x u64 for
+ * Philox4x32 and ARS, 4 x u64 for Threefry4x64; random/increment.hpp:54-104).
+ * `index` counts the words of that block already returned; a value >= words
+ * per block (4 or 8 u32, 2 or 4 u64) means no word is buffered.  The buffered
+ * block itself is not stored: it is a pure function of (key, ctr). */
+typedef struct mckl_b200_engine {
+    uint64_t ctr[4];
+    uint64_t key[4];   /* Philox4x32: 2 x u32; ARS: 4 x u32; Threefry4x64: 4 x u64 */
+    uint64_t tweak[2]; /* Threefry4x64 tweak (ThreefryGenerator::tweak, random/threefry.hpp:126-133) */
+    uint32_t index;
+    uint32_t kind;     /* MCKL_B200_PHILOX4X32 ... MCKL_B200_ARS_64 */
+} mckl_b200_engine_t;
+
+const char *mckl_b200_last_error(void);
+const char *mckl_b200_version(void);
+/* Number of kernels this library has launched in this process (diagnostics;
+ * no counterpart in the reference). */
+uint64_t mckl_b200_launch_count(void);
+
+/* ---- engines (host-only state operations, no GPU work) ------------------ */
+
+/* CounterEngine::seed(s): key = {s, 0, ...}, ctr = 0, nothing buffered
+ * (random/counter.hpp:97-103, 282-287). */
+int mckl_b200_engine_seed(mckl_b200_engine_t *e, uint32_t kind, uint64_t seed);
+/* CounterEngine::discard(nskip) (random/counter.hpp:178-199). */
+int mckl_b200_engine_discard(mckl_b200_engine_t *e, uint64_t nskip);
+
+/* ---- generator-level block kernels --------------------------------------
+ * Same contract as the reference's native kernels
+ * `void mckl_<engine>_<isa>_kernel(uint64_t *ctr, size_t n, void *r, const void *)`
+ * (include/mckl/mckl.h:313-341; call sites random/internal/philox_avx2_4x32.hpp:94-121
+ * and random/internal/aes_aesni_ars.hpp:175-190): n whole blocks for the
+ * counters ctr+1 .. ctr+n are written to r_dev and ctr is advanced by n. */
+int mckl_b200_philox4x32_kernel(uint64_t ctr[2], size_t n, void *r_dev, const uint32_t key[2],
+    void *stream);
+int mckl_b200_threefry4x64_kernel(uint64_t ctr[4], size_t n, void *r_dev, const uint64_t key[4],
+    const uint64_t tweak[2], void *stream);
+int mckl_b200_ars_kernel(uint64_t ctr[2], size_t n, void *r_dev, const uint32_t key[4],
+    void *stream);
+
+/* ---- raw words: mckl::rand(rng, n, r) (random/counter.hpp:142-165, 298-303)
+ * n result words (u32, or u64 for the _64 kinds) into r_dev. */
+int mckl_b200_rand(mckl_b200_engine_t *e, size_t n, void *r_dev, void *stream);
+
+/* ---- U01 distributions (random/u01_distribution.hpp:131-142 and
+ * random/internal/u01_generic.hpp:48-198), reference chunking included:
+ * u01_canonical_distribution / u01_cc / u01_co / u01_oc / u01_oo. */
+int mckl_b200_u01_canonical_f32(mckl_b200_engine_t *e, size_t n, float *r_dev, void *stream);
+int mckl_b200_u01_canonical_f64(mckl_b200_engine_t *e, size_t n, double *r_dev, void *stream);
+int mckl_b200_u01_cc_f32(mckl_b200_engine_t *e, size_t n, float *r_dev, void *stream);
+int mckl_b200_u01_cc_f64(mckl_b200_engine_t *e, size_t n, double *r_dev, void *stream);
+int mckl_b200_u01_co_f32(mckl_b200_engine_t *e, size_t n, float *r_dev, void *stream);
+int mckl_b200_u01_co_f64(mckl_b200_engine_t *e, size_t n, double *r_dev, void *stream);
+int mckl_b200_u01_oc_f32(mckl_b200_engine_t *e, size_t n, float *r_dev, void *stream);
+int mckl_b200_u01_oc_f64(mckl_b200_engine_t *e, size_t n, double *r_dev, void *stream);
+int mckl_b200_u01_oo_f32(mckl_b200_engine_t *e, size_t n, float *r_dev, void *stream);
+int mckl_b200_u01_oo_f64(mckl_b200_engine_t *e, size_t n, double *r_dev, void *stream);
+
+/* Normal: normal_distribution (random/normal_distribution.hpp:50-101): chunks of
+ * 8192 bytes, Box-Muller with the first half of each chunk's uniforms as
+ * radii; an odd n redraws its last value from two further U01OC words. */
+int mckl_b200_normal_f32(mckl_b200_engine_t *e, size_t n, float *r_dev, float mean, float sd,
+    void *stream);
+int mckl_b200_normal_f64(mckl_b200_engine_t *e, size_t n, double *r_dev, double mean, double sd,
+    void *stream);
+
+/* Exponential: exponential_distribution (random/exponential_distribution.hpp:48-60). */
+int mckl_b200_exponential_f32(mckl_b200_engine_t *e, size_t n, float *r_dev, float lambda,
+    void *stream);
+int mckl_b200_exponential_f64(mckl_b200_engine_t *e, size_t n, double *r_dev, double lambda,
+    void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MCKL_B200_H */

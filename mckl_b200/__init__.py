@@ -1,0 +1,347 @@
+"""mckl_b200 -- B200 (sm_100a) implementation of MCKL's counter-based RNG,
+distribution and SMC hot path, reached through the C ABI in
+``include/mckl_b200.h`` (library ``mckl_b200/libmckl_b200.so``).
+
+The Python layer mirrors the reference's interface so tests and benchmarks
+read like the reference's own code:
+
+* engines: :class:`Philox4x32`, :class:`Threefry4x64`, :class:`ARS` and the
+  ``_64`` variants (``mckl::CounterEngine``, random/counter.hpp:61-288) with
+  ``seed`` / ``key`` / ``ctr`` / ``discard``;
+* ``rand(rng, n, r)`` and the batch distributions
+  ``u01_*_distribution``, ``normal_distribution``,
+  ``exponential_distribution``, ``gamma_distribution``
+  (random/internal/common.hpp:69-151);
+* SMC: ``Weight`` (core/weight.hpp), the resampling schemes
+  (algorithm/resample.hpp) and the AR(1) particle filters.
+
+Device memory and streams come from PyTorch tensors; the arithmetic is the
+library's own CUDA.  There is no CPU fallback: importing this package on a
+machine without the built library raises, and calls without a GPU fail.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmckl_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"{LIB_PATH} is missing; build it with `python mckl_b200/build.py` (nvcc, sm_100a)")
+
+_lib = ctypes.CDLL(LIB_PATH)
+
+PHILOX4X32, PHILOX4X32_64, THREEFRY4X64, THREEFRY4X64_64, ARS_KIND, ARS_64_KIND = range(1, 7)
+_WORDS = {1: 4, 2: 2, 3: 8, 4: 4, 5: 4, 6: 2}
+_RESULT_BITS = {1: 32, 2: 64, 3: 32, 4: 64, 5: 32, 6: 64}
+
+
+class MCKLB200Error(RuntimeError):
+    pass
+
+
+class EngineState(ctypes.Structure):
+    """``mckl_b200_engine_t``."""
+
+    _fields_ = [
+        ("ctr", ctypes.c_uint64 * 4),
+        ("key", ctypes.c_uint64 * 4),
+        ("tweak", ctypes.c_uint64 * 2),
+        ("index", ctypes.c_uint32),
+        ("kind", ctypes.c_uint32),
+    ]
+
+
+_vp, _sz, _i, _u32, _u64 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint64
+_f, _d = ctypes.c_float, ctypes.c_double
+_EP = ctypes.POINTER(EngineState)
+
+
+def _bind(name, argtypes, restype=ctypes.c_int):
+    fn = getattr(_lib, name)
+    fn.argtypes = argtypes
+    fn.restype = restype
+    return fn
+
+
+_lib.mckl_b200_last_error.restype = ctypes.c_char_p
+_lib.mckl_b200_version.restype = ctypes.c_char_p
+_lib.mckl_b200_launch_count.restype = ctypes.c_uint64
+_engine_seed = _bind("mckl_b200_engine_seed", [_EP, _u32, _u64])
+_engine_discard = _bind("mckl_b200_engine_discard", [_EP, _u64])
+_rand = _bind("mckl_b200_rand", [_EP, _sz, _vp, _vp])
+_philox_kernel = _bind("mckl_b200_philox4x32_kernel", [_vp, _sz, _vp, _vp, _vp])
+_threefry_kernel = _bind("mckl_b200_threefry4x64_kernel", [_vp, _sz, _vp, _vp, _vp, _vp])
+_ars_kernel = _bind("mckl_b200_ars_kernel", [_vp, _sz, _vp, _vp, _vp])
+_u01 = {}
+for _name in ("canonical", "cc", "co", "oc", "oo"):
+    for _t in ("f32", "f64"):
+        _u01[(_name, _t)] = _bind(f"mckl_b200_u01_{_name}_{_t}", [_EP, _sz, _vp, _vp])
+_normal = {"f32": _bind("mckl_b200_normal_f32", [_EP, _sz, _vp, _f, _f, _vp]),
+           "f64": _bind("mckl_b200_normal_f64", [_EP, _sz, _vp, _d, _d, _vp])}
+_exponential = {"f32": _bind("mckl_b200_exponential_f32", [_EP, _sz, _vp, _f, _vp]),
+                "f64": _bind("mckl_b200_exponential_f64", [_EP, _sz, _vp, _d, _vp])}
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise MCKLB200Error(f"mckl_b200 error {rc}: {_lib.mckl_b200_last_error().decode()}")
+
+
+def version() -> str:
+    return _lib.mckl_b200_version().decode()
+
+
+def launch_count() -> int:
+    """Kernels launched by the library so far in this process."""
+    return int(_lib.mckl_b200_launch_count())
+
+
+def lib_path() -> str:
+    return LIB_PATH
+
+
+def raw_lib() -> ctypes.CDLL:
+    """The loaded C-ABI library (for callers binding further entry points)."""
+    return _lib
+
+
+# ---------------------------------------------------------------------------
+# engines
+# ---------------------------------------------------------------------------
+class CounterEngine:
+    """Host handle of one counter-based engine (``mckl::CounterEngine``).
+
+    The state lives on the host and is advanced by every call exactly as the
+    reference engine's would be; the words themselves are produced on the GPU.
+    """
+
+    kind = 0
+
+    def __init__(self, seed: int = 1, key=None):
+        self.state = EngineState()
+        self.seed(seed)
+        if key is not None:
+            self.key = key
+
+    # -- reference API ----------------------------------------------------
+    def seed(self, s: int) -> None:
+        _check(_engine_seed(ctypes.byref(self.state), self.kind, int(s)))
+
+    @property
+    def key(self):
+        n = 2 if self.kind in (PHILOX4X32, PHILOX4X32_64) else 4
+        return tuple(int(self.state.key[i]) for i in range(n))
+
+    @key.setter
+    def key(self, k) -> None:
+        # CounterEngine::key(k) == seed(k): counter reset, nothing buffered
+        for i in range(4):
+            self.state.key[i] = int(k[i]) if i < len(k) else 0
+        for i in range(4):
+            self.state.ctr[i] = 0
+        self.state.index = _WORDS[self.kind]
+
+    @property
+    def ctr(self):
+        n = 4 if self.kind in (THREEFRY4X64, THREEFRY4X64_64) else 2
+        return tuple(int(self.state.ctr[i]) for i in range(n))
+
+    @ctr.setter
+    def ctr(self, c) -> None:
+        # CounterEngine::ctr(c): set the counter, drop the buffer (random/counter.hpp:129-133)
+        for i in range(4):
+            self.state.ctr[i] = int(c[i]) if i < len(c) else 0
+        self.state.index = _WORDS[self.kind]
+
+    @property
+    def index(self) -> int:
+        return int(self.state.index)
+
+    def discard(self, nskip: int) -> None:
+        _check(_engine_discard(ctypes.byref(self.state), int(nskip)))
+
+    def words_per_block(self) -> int:
+        return _WORDS[self.kind]
+
+    def result_bits(self) -> int:
+        return _RESULT_BITS[self.kind]
+
+    def copy(self):
+        other = type(self).__new__(type(self))
+        other.state = EngineState()
+        ctypes.pointer(other.state)[0] = self.state
+        return other
+
+    def state_tuple(self):
+        s = self.state
+        return (tuple(s.ctr), tuple(s.key), tuple(s.tweak), int(s.index), int(s.kind))
+
+    def load_state(self, ctr, key, tweak, index) -> None:
+        for i in range(4):
+            self.state.ctr[i] = int(ctr[i])
+            self.state.key[i] = int(key[i])
+        self.state.tweak[0], self.state.tweak[1] = int(tweak[0]), int(tweak[1])
+        self.state.index = int(index)
+
+
+class Philox4x32(CounterEngine):
+    kind = PHILOX4X32
+
+
+class Philox4x32_64(CounterEngine):
+    kind = PHILOX4X32_64
+
+
+class Threefry4x64(CounterEngine):
+    kind = THREEFRY4X64
+
+    def tweak(self, t0: int, t1: int) -> None:
+        self.state.tweak[0], self.state.tweak[1] = int(t0), int(t1)
+
+
+class Threefry4x64_64(Threefry4x64):
+    kind = THREEFRY4X64_64
+
+
+class ARS(CounterEngine):
+    kind = ARS_KIND
+
+
+class ARS_64(CounterEngine):
+    kind = ARS_64_KIND
+
+
+ENGINES = {"Philox4x32": Philox4x32, "Philox4x32_64": Philox4x32_64, "Threefry4x64": Threefry4x64,
+           "Threefry4x64_64": Threefry4x64_64, "ARS": ARS, "ARS_64": ARS_64}
+
+
+# ---------------------------------------------------------------------------
+# tensors and streams
+# ---------------------------------------------------------------------------
+def _torch():
+    import torch  # local: the library itself does not need torch
+
+    return torch
+
+
+def _stream_ptr(stream=None) -> int:
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+def _check_out(r, n: int, itemsize: int):
+    torch = _torch()
+    if not isinstance(r, torch.Tensor) or not (r.is_cuda or r.is_pinned()):
+        raise MCKLB200Error("output must be a CUDA tensor or a pinned host tensor")
+    if not r.is_contiguous() or r.element_size() != itemsize or r.numel() < n:
+        raise MCKLB200Error("output tensor has the wrong size, dtype width or layout")
+    return ctypes.c_void_p(r.data_ptr())
+
+
+def empty_words(rng: CounterEngine, n: int, device="cuda"):
+    torch = _torch()
+    return torch.empty(n, dtype=torch.int64 if rng.result_bits() == 64 else torch.int32, device=device)
+
+
+# ---------------------------------------------------------------------------
+# RNG and distributions (reference batch calls)
+# ---------------------------------------------------------------------------
+def rand(rng: CounterEngine, n: int, r=None, stream=None):
+    """``mckl::rand(rng, n, r)``: n raw result words (int32/int64 tensor bits)."""
+    if r is None:
+        r = empty_words(rng, n)
+    ptr = _check_out(r, n, rng.result_bits() // 8)
+    _check(_rand(ctypes.byref(rng.state), n, ptr, _stream_ptr(stream)))
+    return r
+
+
+def _real_out(r, n, dtype):
+    torch = _torch()
+    if r is None:
+        r = torch.empty(n, dtype=torch.float64 if dtype == "f64" else torch.float32, device="cuda")
+    t = "f64" if r.dtype == torch.float64 else "f32"
+    if t != dtype and dtype is not None:
+        raise MCKLB200Error("output dtype mismatch")
+    return r, t
+
+
+def _u01_call(variant, rng, n, r, dtype, stream):
+    r, t = _real_out(r, n, dtype)
+    ptr = _check_out(r, n, 8 if t == "f64" else 4)
+    _check(_u01[(variant, t)](ctypes.byref(rng.state), n, ptr, _stream_ptr(stream)))
+    return r
+
+
+def u01_canonical_distribution(rng, n, r=None, dtype="f64", stream=None):
+    return _u01_call("canonical", rng, n, r, None if r is not None else dtype, stream)
+
+
+u01_distribution = u01_canonical_distribution
+
+
+def u01_cc_distribution(rng, n, r=None, dtype="f64", stream=None):
+    return _u01_call("cc", rng, n, r, None if r is not None else dtype, stream)
+
+
+def u01_co_distribution(rng, n, r=None, dtype="f64", stream=None):
+    return _u01_call("co", rng, n, r, None if r is not None else dtype, stream)
+
+
+def u01_oc_distribution(rng, n, r=None, dtype="f64", stream=None):
+    return _u01_call("oc", rng, n, r, None if r is not None else dtype, stream)
+
+
+def u01_oo_distribution(rng, n, r=None, dtype="f64", stream=None):
+    return _u01_call("oo", rng, n, r, None if r is not None else dtype, stream)
+
+
+def normal_distribution(rng, n, r=None, mean=0.0, stddev=1.0, dtype="f64", stream=None):
+    r, t = _real_out(r, n, None if r is not None else dtype)
+    ptr = _check_out(r, n, 8 if t == "f64" else 4)
+    _check(_normal[t](ctypes.byref(rng.state), n, ptr, mean, stddev, _stream_ptr(stream)))
+    return r
+
+
+def exponential_distribution(rng, n, r=None, lam=1.0, dtype="f64", stream=None):
+    r, t = _real_out(r, n, None if r is not None else dtype)
+    ptr = _check_out(r, n, 8 if t == "f64" else 4)
+    _check(_exponential[t](ctypes.byref(rng.state), n, ptr, lam, _stream_ptr(stream)))
+    return r
+
+
+def philox4x32_kernel(ctr, n, r, key, stream=None):
+    """Generator-level kernel: n blocks for counters ctr+1..ctr+n; returns new ctr."""
+    c = (ctypes.c_uint64 * 2)(*[int(x) for x in ctr])
+    k = (ctypes.c_uint32 * 2)(*[int(x) for x in key])
+    _check(_philox_kernel(ctypes.cast(c, _vp), n, _check_out(r, n * 4, 4), ctypes.cast(k, _vp),
+                          _stream_ptr(stream)))
+    return (int(c[0]), int(c[1]))
+
+
+def threefry4x64_kernel(ctr, n, r, key, tweak=(0, 0), stream=None):
+    c = (ctypes.c_uint64 * 4)(*[int(x) for x in ctr])
+    k = (ctypes.c_uint64 * 4)(*[int(x) for x in key])
+    t = (ctypes.c_uint64 * 2)(*[int(x) for x in tweak])
+    _check(_threefry_kernel(ctypes.cast(c, _vp), n, _check_out(r, n * 8, 4), ctypes.cast(k, _vp),
+                            ctypes.cast(t, _vp), _stream_ptr(stream)))
+    return tuple(int(x) for x in c)
+
+
+def ars_kernel(ctr, n, r, key, stream=None):
+    c = (ctypes.c_uint64 * 2)(*[int(x) for x in ctr])
+    k = (ctypes.c_uint32 * 4)(*[int(x) for x in key])
+    _check(_ars_kernel(ctypes.cast(c, _vp), n, _check_out(r, n * 4, 4), ctypes.cast(k, _vp),
+                       _stream_ptr(stream)))
+    return (int(c[0]), int(c[1]))
+
+
+def words_to_numpy(t, bits: int) -> np.ndarray:
+    """Copy a device word tensor to a numpy array of unsigned words."""
+    a = t.cpu().numpy()
+    return a.view(np.uint64 if bits == 64 else np.uint32)

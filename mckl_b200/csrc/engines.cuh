@@ -1,0 +1,321 @@
+// engines.cuh -- sm_100a device implementations of MCKL's three counter-based
+// generators.  Each generator maps one counter to one block of random words;
+// no state is carried between blocks, so any thread can produce any block of
+// any stream from (key, counter) alone.
+//
+//   Philox4x32-10   random/internal/philox_generic_4x.hpp:40-53,
+//                   random/internal/philox_constants.hpp:51-56, 82-87
+//   Threefry4x64-20 random/threefry.hpp:109-133,
+//                   random/internal/threefry_common.hpp:212-247,
+//                   random/internal/threefry_generic_4x64.hpp:40-79,
+//                   random/internal/threefry_constants.hpp:51-56, 83-89
+//   ARS-5           random/internal/aes_generic.hpp:254-306, 413-491,
+//                   random/internal/aes_constants.hpp:289-304
+//
+// Block words are little-endian u32: a Philox/ARS block is 4 words, a
+// Threefry4x64 block is 8 words (lo, hi of each 64-bit lane).  Engines with
+// 64-bit results read the same bytes two words at a time.
+#pragma once
+
+#include <cstdint>
+
+namespace mckl_b200 {
+
+// 128/256-bit counters in the reference's Counter layout (random/increment.hpp:54-104).
+struct Ctr {
+    uint64_t w[4];
+};
+
+__host__ __device__ inline Ctr ctr_add(const Ctr &c, uint64_t k, int nwords)
+{
+    Ctr r = c;
+    uint64_t s = r.w[0] + k;
+    uint64_t carry = (s < r.w[0]) ? 1 : 0;
+    r.w[0] = s;
+    for (int i = 1; i < nwords && carry; ++i) {
+        r.w[i] += 1;
+        carry = (r.w[i] == 0) ? 1 : 0;
+    }
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10
+// ---------------------------------------------------------------------------
+struct PhiloxGen {
+    static constexpr int kWords = 4;     // u32 words per block
+    static constexpr int kCtrWords = 2;  // u64 counter words
+    static constexpr int kDynSmem = 0;   // dynamic shared memory bytes per CTA
+    uint32_t k0, k1;
+
+    __device__ __forceinline__ void prepare() const {}
+
+    __device__ __forceinline__ void block(const Ctr &c, uint32_t out[4]) const
+    {
+        uint32_t s0 = static_cast<uint32_t>(c.w[0]);
+        uint32_t s1 = static_cast<uint32_t>(c.w[0] >> 32);
+        uint32_t s2 = static_cast<uint32_t>(c.w[1]);
+        uint32_t s3 = static_cast<uint32_t>(c.w[1] >> 32);
+        uint32_t a = k0, b = k1;
+#pragma unroll
+        for (int r = 0; r < 10; ++r) {
+            const uint32_t hi2 = __umulhi(s2, 0xCD9E8D57u);
+            const uint32_t lo2 = s2 * 0xCD9E8D57u;
+            const uint32_t hi0 = __umulhi(s0, 0xD2511F53u);
+            const uint32_t lo0 = s0 * 0xD2511F53u;
+            s0 = a ^ s1 ^ hi2;
+            s1 = lo2;
+            s2 = b ^ s3 ^ hi0;
+            s3 = lo0;
+            a += 0x9E3779B9u;
+            b += 0xBB67AE85u;
+        }
+        out[0] = s0;
+        out[1] = s1;
+        out[2] = s2;
+        out[3] = s3;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Threefry4x64-20.  The key-injection words of all six injections are
+// precomputed on the host (they do not depend on the counter).
+// ---------------------------------------------------------------------------
+struct ThreefryGen {
+    static constexpr int kWords = 8;
+    static constexpr int kCtrWords = 4;
+    static constexpr int kDynSmem = 0;
+    uint64_t inj[6][4];  // inj[S][i] = par[(S+i)%5] + tweak/parity terms, S = round/4
+
+    __host__ static ThreefryGen make(const uint64_t key[4], const uint64_t tweak[2])
+    {
+        ThreefryGen g;
+        uint64_t par[8];
+        for (int i = 0; i < 4; ++i) par[i] = key[i];
+        par[4] = 0x1BD11BDAA9FC1A22ull ^ key[0] ^ key[1] ^ key[2] ^ key[3];
+        par[5] = tweak[0];
+        par[6] = tweak[1];
+        par[7] = tweak[0] ^ tweak[1];
+        for (uint64_t S = 0; S < 6; ++S) {
+            g.inj[S][0] = par[(S + 0) % 5];
+            g.inj[S][1] = par[(S + 1) % 5] + par[5 + (S + 0) % 3];
+            g.inj[S][2] = par[(S + 2) % 5] + par[5 + (S + 1) % 3];
+            g.inj[S][3] = par[(S + 3) % 5] + S;
+        }
+        return g;
+    }
+
+    __device__ __forceinline__ void prepare() const {}
+
+    template <int L>
+    __device__ __forceinline__ static uint64_t rotl(uint64_t x)
+    {
+        if constexpr (L == 32) {
+            return (x << 32) | (x >> 32);
+        } else {
+            return (x << L) | (x >> (64 - L));
+        }
+    }
+
+    template <int L0, int L1>
+    __device__ __forceinline__ static void round(uint64_t &s0, uint64_t &s1, uint64_t &s2,
+        uint64_t &s3)
+    {
+        s0 += s1;
+        s2 += s3;
+        const uint64_t t1 = rotl<L0>(s1);
+        const uint64_t t3 = rotl<L1>(s3);
+        s1 = s2 ^ t3;
+        s3 = s0 ^ t1;
+    }
+
+    __device__ __forceinline__ void inject(int S, uint64_t &s0, uint64_t &s1, uint64_t &s2,
+        uint64_t &s3) const
+    {
+        s0 += inj[S][0];
+        s1 += inj[S][1];
+        s2 += inj[S][2];
+        s3 += inj[S][3];
+    }
+
+    __device__ __forceinline__ void block(const Ctr &c, uint32_t out[8]) const
+    {
+        uint64_t s0 = c.w[0], s1 = c.w[1], s2 = c.w[2], s3 = c.w[3];
+        inject(0, s0, s1, s2, s3);
+#pragma unroll
+        for (int cyc = 0; cyc < 5; ++cyc) {
+            if (cyc % 2 == 0) {
+                round<14, 16>(s0, s1, s2, s3);
+                round<52, 57>(s0, s1, s2, s3);
+                round<23, 40>(s0, s1, s2, s3);
+                round<5, 37>(s0, s1, s2, s3);
+            } else {
+                round<25, 33>(s0, s1, s2, s3);
+                round<46, 12>(s0, s1, s2, s3);
+                round<58, 22>(s0, s1, s2, s3);
+                round<32, 32>(s0, s1, s2, s3);
+            }
+            inject(cyc + 1, s0, s1, s2, s3);
+        }
+        out[0] = static_cast<uint32_t>(s0);
+        out[1] = static_cast<uint32_t>(s0 >> 32);
+        out[2] = static_cast<uint32_t>(s1);
+        out[3] = static_cast<uint32_t>(s1 >> 32);
+        out[4] = static_cast<uint32_t>(s2);
+        out[5] = static_cast<uint32_t>(s2 >> 32);
+        out[6] = static_cast<uint32_t>(s3);
+        out[7] = static_cast<uint32_t>(s3 >> 32);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// ARS-5 with table-driven AES rounds from shared memory.
+//
+// The AES S-box and the round table Te0 (Te0[x] = {2S(x), S(x), S(x), 3S(x)}
+// as little-endian bytes) are derived at compile time from GF(2^8)
+// arithmetic.  In shared memory Te0 is replicated once per lane
+// (tab[x * 32 + lane]), so the 32 lanes of a warp always hit 32 different
+// banks; Te1..Te3 are byte rotations of Te0 and the final-round S-box byte is
+// byte 1 of Te0.
+// ---------------------------------------------------------------------------
+struct AesTables {
+    uint32_t te0[256];
+};
+
+constexpr uint8_t gf_mul(uint8_t a, uint8_t b)
+{
+    uint8_t p = 0;
+    for (int i = 0; i < 8; ++i) {
+        if (b & 1) p = static_cast<uint8_t>(p ^ a);
+        const bool hi = (a & 0x80) != 0;
+        a = static_cast<uint8_t>(a << 1);
+        if (hi) a = static_cast<uint8_t>(a ^ 0x1B);
+        b = static_cast<uint8_t>(b >> 1);
+    }
+    return p;
+}
+
+constexpr uint8_t gf_inv(uint8_t x)
+{
+    // x^254 by square-and-multiply (0 maps to 0)
+    uint8_t r = 1, base = x;
+    int e = 254;
+    while (e) {
+        if (e & 1) r = gf_mul(r, base);
+        base = gf_mul(base, base);
+        e >>= 1;
+    }
+    return x == 0 ? 0 : r;
+}
+
+constexpr uint8_t aes_sbox_entry(int x)
+{
+    uint8_t b = gf_inv(static_cast<uint8_t>(x));
+    uint8_t s = b;
+    for (int i = 0; i < 4; ++i) {
+        b = static_cast<uint8_t>((b << 1) | (b >> 7));
+        s = static_cast<uint8_t>(s ^ b);
+    }
+    return static_cast<uint8_t>(s ^ 0x63);
+}
+
+constexpr AesTables make_aes_tables()
+{
+    AesTables t{};
+    for (int x = 0; x < 256; ++x) {
+        const uint8_t s = aes_sbox_entry(x);
+        t.te0[x] = static_cast<uint32_t>(gf_mul(s, 2)) | (static_cast<uint32_t>(s) << 8) |
+                   (static_cast<uint32_t>(s) << 16) | (static_cast<uint32_t>(gf_mul(s, 3)) << 24);
+    }
+    return t;
+}
+
+__constant__ const AesTables kAesTables = make_aes_tables();
+
+// The lane-replicated table lives at the start of the kernel's dynamic shared
+// memory; every kernel instantiated with ArsGen is launched with
+// ArsGen::kDynSmem bytes of it.
+__device__ __forceinline__ uint32_t *ars_smem_table()
+{
+    extern __shared__ __align__(16) uint32_t mb_dyn_smem[];
+    return mb_dyn_smem;
+}
+
+struct ArsGen {
+    static constexpr int kWords = 4;
+    static constexpr int kCtrWords = 2;
+    static constexpr int kDynSmem = 256 * 32 * 4;
+    uint32_t rk[6][4];
+
+    __host__ static ArsGen make(const uint64_t key[4])
+    {
+        ArsGen g;
+        const uint64_t klo = (key[0] & 0xFFFFFFFFull) | ((key[1] & 0xFFFFFFFFull) << 32);
+        const uint64_t khi = (key[2] & 0xFFFFFFFFull) | ((key[3] & 0xFFFFFFFFull) << 32);
+        for (uint64_t n = 0; n <= 5; ++n) {
+            const uint64_t a = klo + 0x9E3779B97F4A7C15ull * n;
+            const uint64_t b = khi + 0xBB67AE8584CAA73Bull * n;
+            g.rk[n][0] = static_cast<uint32_t>(a);
+            g.rk[n][1] = static_cast<uint32_t>(a >> 32);
+            g.rk[n][2] = static_cast<uint32_t>(b);
+            g.rk[n][3] = static_cast<uint32_t>(b >> 32);
+        }
+        return g;
+    }
+
+    // Every thread of the CTA must call prepare() before the first block().
+    __device__ __forceinline__ void prepare() const
+    {
+        uint32_t *tab = ars_smem_table();
+        for (int i = threadIdx.x; i < 256 * 32; i += blockDim.x) {
+            tab[i] = kAesTables.te0[i >> 5];
+        }
+        __syncthreads();
+    }
+
+    __device__ __forceinline__ static uint32_t lookup(const uint32_t *lane_tab, uint32_t byte)
+    {
+        return lane_tab[byte << 5];
+    }
+
+    __device__ __forceinline__ static uint32_t rot(uint32_t x, int r)
+    {
+        return __funnelshift_l(x, x, r);
+    }
+
+    __device__ __forceinline__ void block(const Ctr &c, uint32_t out[4]) const
+    {
+        const uint32_t *lt = ars_smem_table() + (threadIdx.x & 31);
+        uint32_t s0 = static_cast<uint32_t>(c.w[0]) ^ rk[0][0];
+        uint32_t s1 = static_cast<uint32_t>(c.w[0] >> 32) ^ rk[0][1];
+        uint32_t s2 = static_cast<uint32_t>(c.w[1]) ^ rk[0][2];
+        uint32_t s3 = static_cast<uint32_t>(c.w[1] >> 32) ^ rk[0][3];
+#pragma unroll
+        for (int r = 1; r <= 4; ++r) {
+            const uint32_t t0 = rk[r][0] ^ lookup(lt, s0 & 0xFF) ^ rot(lookup(lt, (s1 >> 8) & 0xFF), 8) ^
+                                rot(lookup(lt, (s2 >> 16) & 0xFF), 16) ^ rot(lookup(lt, s3 >> 24), 24);
+            const uint32_t t1 = rk[r][1] ^ lookup(lt, s1 & 0xFF) ^ rot(lookup(lt, (s2 >> 8) & 0xFF), 8) ^
+                                rot(lookup(lt, (s3 >> 16) & 0xFF), 16) ^ rot(lookup(lt, s0 >> 24), 24);
+            const uint32_t t2 = rk[r][2] ^ lookup(lt, s2 & 0xFF) ^ rot(lookup(lt, (s3 >> 8) & 0xFF), 8) ^
+                                rot(lookup(lt, (s0 >> 16) & 0xFF), 16) ^ rot(lookup(lt, s1 >> 24), 24);
+            const uint32_t t3 = rk[r][3] ^ lookup(lt, s3 & 0xFF) ^ rot(lookup(lt, (s0 >> 8) & 0xFF), 8) ^
+                                rot(lookup(lt, (s1 >> 16) & 0xFF), 16) ^ rot(lookup(lt, s2 >> 24), 24);
+            s0 = t0;
+            s1 = t1;
+            s2 = t2;
+            s3 = t3;
+        }
+        // last round: S-box bytes (byte 1 of Te0) in ShiftRows order
+        auto sb = [lt](uint32_t byte) -> uint32_t { return (lookup(lt, byte) >> 8) & 0xFF; };
+        out[0] = rk[5][0] ^ sb(s0 & 0xFF) ^ (sb((s1 >> 8) & 0xFF) << 8) ^ (sb((s2 >> 16) & 0xFF) << 16) ^
+                 (sb(s3 >> 24) << 24);
+        out[1] = rk[5][1] ^ sb(s1 & 0xFF) ^ (sb((s2 >> 8) & 0xFF) << 8) ^ (sb((s3 >> 16) & 0xFF) << 16) ^
+                 (sb(s0 >> 24) << 24);
+        out[2] = rk[5][2] ^ sb(s2 & 0xFF) ^ (sb((s3 >> 8) & 0xFF) << 8) ^ (sb((s0 >> 16) & 0xFF) << 16) ^
+                 (sb(s1 >> 24) << 24);
+        out[3] = rk[5][3] ^ sb(s3 & 0xFF) ^ (sb((s0 >> 8) & 0xFF) << 8) ^ (sb((s1 >> 16) & 0xFF) << 16) ^
+                 (sb(s2 >> 24) << 24);
+    }
+};
+
+}  // namespace mckl_b200

@@ -25,6 +25,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmckl_ref.so")
+REF_GENERIC_SO = os.path.join(HERE, "_ref", "libmckl_ref_generic.so")
 REF_ROOT = "/root/reference"
 
 PHILOX4X32, PHILOX4X32_64, THREEFRY4X64, THREEFRY4X64_64, ARS, ARS_64 = range(1, 7)
@@ -80,8 +81,10 @@ class CPUPath:
     """Uniform wrapper over ``orc_*`` (restatement) or ``ref_*`` (reference)."""
 
     def __init__(self, which: str = "oracle"):
+        """which: "oracle" (restatement), "ref" (reference, AES-NI paths on) or
+        "ref_generic" (reference with its generic ARS path)."""
         self.which = which
-        path = ORACLE_SO if which == "oracle" else REF_SO
+        path = {"oracle": ORACLE_SO, "ref": REF_SO, "ref_generic": REF_GENERIC_SO}[which]
         if not os.path.exists(path):
             raise FileNotFoundError(path)
         self.lib = ctypes.CDLL(path)
@@ -242,4 +245,4 @@ class CPUPath:
 
 
 def have_ref() -> bool:
-    return os.path.exists(REF_SO)
+    return os.path.exists(REF_SO) and os.path.exists(REF_GENERIC_SO)
