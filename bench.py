@@ -232,7 +232,27 @@ def bench_rng(args, rank, world, dev):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_elapsed = float(t.item())
     e2e_value = world * bytes_per_step * e2e_steps / e2e_elapsed / 1e9
+    # Philox4x32 configuration: 2^26 raw words, then 2^24 U01OO doubles from the same stream
+    g = mb.Philox4x32(42)
+    p32 = torch.empty(1 << 26, dtype=torch.int32, device=dev)
+    p64 = torch.empty(1 << 24, dtype=torch.float64, device=dev)
+    for _ in range(3):
+        mb.rand(mb.Philox4x32(42), 1 << 26, p32)
+    c1 = {}
+    for name, fn, nbytes in (("rand_u32_2^26", lambda gg: mb.rand(gg, 1 << 26, p32), 4 << 26),
+                             ("u01oo_f64_2^24", lambda gg: mb.u01_oo_distribution(gg, 1 << 24, p64), 8 << 24)):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        reps = 50
+        a.record(stream)
+        for _ in range(reps):
+            fn(mb.Philox4x32(42))
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / reps
+        c1[name] = {"ms": round(ms, 4), "GB_s": round(nbytes / (ms / 1e3) / 1e9, 1)}
     return dict(value=value, elapsed=elapsed, bytes_per_step=bytes_per_step, per_op=per_op, dominant=dominant,
+                philox_c1=c1,
                 clocks=clk, launches=launches, e2e=dict(value=e2e_value, unit="GB/s", h2d_bytes_per_step=0,
                                                         d2h_bytes_per_step=bytes_per_step,
                                                         note="kernels write page-locked host buffers directly"))
@@ -329,6 +349,7 @@ def main():
                      "traffic": None},
         "e2e": res["e2e"], "gpu_launches": res["launches"], "clocks": res["clocks"],
         "per_op": {k: {"ms": round(v["ms"], 4), "GB_s": round(v["GB_s"], 1)} for k, v in res["per_op"].items()},
+        "philox4x32_config": res["philox_c1"],
     }
     if rank == 0 and world == 1:
         cb = cpu_rng_baseline(sample_log2=24)

@@ -117,6 +117,11 @@ int mckl_b200_exponential_f32(mckl_b200_engine_t *e, size_t n, float *r_dev, flo
 int mckl_b200_exponential_f64(mckl_b200_engine_t *e, size_t n, double *r_dev, double lambda,
     void *stream);
 
+/* ---- diagnostics (no counterpart in the reference) ----------------------
+ * The library's double-double log (fn 0), exp (fn 1) and sin/cos (fn 2; cos
+ * into y2_dev when non-null) element-wise, for checking against a host libm. */
+int mckl_b200_math_f64(int fn, size_t n, const double *x_dev, double *y_dev, double *y2_dev, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -87,6 +87,20 @@ _exponential = {"f32": _bind("mckl_b200_exponential_f32", [_EP, _sz, _vp, _f, _v
                 "f64": _bind("mckl_b200_exponential_f64", [_EP, _sz, _vp, _d, _vp])}
 
 
+_math_f64 = _bind("mckl_b200_math_f64", [_i, _sz, _vp, _vp, _vp, _vp])
+
+
+def math_f64(fn: str, x):
+    """The library's double-double log / exp / sincos on a CUDA float64 tensor."""
+    torch = _torch()
+    code = {"log": 0, "exp": 1, "sincos": 2}[fn]
+    y = torch.empty_like(x)
+    y2 = torch.empty_like(x) if code == 2 else None
+    _check(_math_f64(code, x.numel(), ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(y.data_ptr()),
+                     ctypes.c_void_p(y2.data_ptr()) if y2 is not None else None, _stream_ptr()))
+    return (y, y2) if code == 2 else y
+
+
 def _check(rc: int) -> None:
     if rc != 0:
         raise MCKLB200Error(f"mckl_b200 error {rc}: {_lib.mckl_b200_last_error().decode()}")

@@ -1,0 +1,327 @@
+// crmath.cuh -- double-precision log, exp and sin/cos evaluated in
+// double-double arithmetic and rounded once, so the result is the correctly
+// rounded value except when the exact result lies within ~2^-70 relative of
+// a rounding midpoint.
+//
+// Why: the reference's transforms call glibc's log/exp/sin/cos, which are
+// correctly rounded in all but rare cases.  CUDA's library versions are
+// accurate to 1-2 ULP, and Box-Muller's sqrt(-2 log u) * sin(2 pi v) compounds
+// those into 3-ULP differences.  Evaluating in double-double makes the device
+// agree with the reference to within its own rounding.
+//
+// Methods (standard, written from the mathematics):
+//   log: x = 2^e m, m in [1/sqrt2, sqrt2); log m = 2 atanh(z), z = (m-1)/(m+1),
+//        atanh series in z^2 (|z| <= 0.1716) with its first terms in
+//        double-double; e ln2 with ln2 as a double-double constant.
+//   exp: x = k ln2 + r (Cody-Waite, three-part ln2), r/16 through a Taylor
+//        series for expm1 in double-double, four squarings of 1 + expm1,
+//        scaled by 2^k.
+//   sin/cos: x = k pi/2 + r (Cody-Waite with four parts of pi/2, |x| < 1e5),
+//        Taylor series of sin r and cos r (|r| <= pi/4) with the leading
+//        terms in double-double; the quadrant picks signs and swaps.
+// Constants are the exact double / double-double splits of ln 2, pi/2 and the
+// series coefficients.
+#pragma once
+
+#include <cstdint>
+
+// The same source compiles for the device (CUDA intrinsics, explicit
+// round-to-nearest) and for a host check against the C library (plain
+// operators; the host build must use -ffp-contract=off).
+#if defined(__CUDACC__)
+#define MB_HD __host__ __device__ __forceinline__
+#else
+#include <cmath>
+#include <cstring>
+#define MB_HD inline
+#endif
+
+#if defined(__CUDA_ARCH__)
+#define MB_ADD(a, b) __dadd_rn((a), (b))
+#define MB_SUB(a, b) __dsub_rn((a), (b))
+#define MB_MUL(a, b) __dmul_rn((a), (b))
+#define MB_DIV(a, b) __ddiv_rn((a), (b))
+#define MB_FMA(a, b, c) __fma_rn((a), (b), (c))
+#define MB_RINT(a) rint(a)
+#define MB_AS_BITS(x) __double_as_longlong(x)
+#define MB_FROM_BITS(b) __longlong_as_double(b)
+#define MB_LIB_SINCOS(x, s, c) ::sincos((x), (s), (c))
+#else
+#define MB_ADD(a, b) ((a) + (b))
+#define MB_SUB(a, b) ((a) - (b))
+#define MB_MUL(a, b) ((a) * (b))
+#define MB_DIV(a, b) ((a) / (b))
+#define MB_FMA(a, b, c) std::fma((a), (b), (c))
+#define MB_RINT(a) std::rint(a)
+#define MB_AS_BITS(x) ::mckl_b200::dd::host_bits(x)
+#define MB_FROM_BITS(b) ::mckl_b200::dd::host_double(b)
+#define MB_LIB_SINCOS(x, s, c) (*(s) = std::sin(x), *(c) = std::cos(x))
+#endif
+
+namespace mckl_b200 {
+namespace dd {
+
+#if !defined(__CUDA_ARCH__)
+inline long long host_bits(double x)
+{
+    long long b;
+    std::memcpy(&b, &x, sizeof(b));
+    return b;
+}
+inline double host_double(long long b)
+{
+    double x;
+    std::memcpy(&x, &b, sizeof(x));
+    return x;
+}
+#endif
+
+struct DD {
+    double hi, lo;
+};
+
+MB_HD DD two_sum(double a, double b)
+{
+    const double s = MB_ADD(a, b);
+    const double bb = MB_SUB(s, a);
+    const double err = MB_ADD(MB_SUB(a, MB_SUB(s, bb)), MB_SUB(b, bb));
+    return {s, err};
+}
+
+MB_HD DD fast_two_sum(double a, double b)
+{
+    const double s = MB_ADD(a, b);
+    return {s, MB_SUB(b, MB_SUB(s, a))};
+}
+
+MB_HD DD two_prod(double a, double b)
+{
+    const double p = MB_MUL(a, b);
+    return {p, MB_FMA(a, b, -p)};
+}
+
+MB_HD DD add(DD a, DD b)
+{
+    DD s = two_sum(a.hi, b.hi);
+    const DD t = two_sum(a.lo, b.lo);
+    s.lo = MB_ADD(s.lo, t.hi);
+    s = fast_two_sum(s.hi, s.lo);
+    s.lo = MB_ADD(s.lo, t.lo);
+    return fast_two_sum(s.hi, s.lo);
+}
+
+MB_HD DD add_d(DD a, double b)
+{
+    DD s = two_sum(a.hi, b);
+    s.lo = MB_ADD(s.lo, a.lo);
+    return fast_two_sum(s.hi, s.lo);
+}
+
+MB_HD DD mul(DD a, DD b)
+{
+    DD p = two_prod(a.hi, b.hi);
+    p.lo = MB_FMA(a.hi, b.lo, p.lo);
+    p.lo = MB_FMA(a.lo, b.hi, p.lo);
+    return fast_two_sum(p.hi, p.lo);
+}
+
+MB_HD DD mul_d(DD a, double b)
+{
+    DD p = two_prod(a.hi, b);
+    p.lo = MB_FMA(a.lo, b, p.lo);
+    return fast_two_sum(p.hi, p.lo);
+}
+
+// ---------------------------------------------------------------------------
+constexpr double kLn2Hi = 0x1.62e42fefa39efp-1, kLn2Lo = 0x1.abc9e3b39803fp-56;
+constexpr double kThirdHi = 0x1.5555555555555p-2, kThirdLo = 0x1.5555555555555p-56;
+constexpr double kSqrt2 = 0x1.6a09e667f3bcdp+0;
+
+// Correctly rounded (see header) natural logarithm of a double.
+MB_HD double log(double x)
+{
+    if (!(x > 0.0)) return x == 0.0 ? -MB_FROM_BITS(0x7ff0000000000000ll) : MB_FROM_BITS(0x7ff8000000000000ll);
+    long long bits = MB_AS_BITS(x);
+    int ex = static_cast<int>((bits >> 52) & 0x7ff);
+    if (ex == 0x7ff) return x;  // +inf
+    int e;
+    if (ex == 0) {  // subnormal: scale into the normal range
+        bits = MB_AS_BITS(MB_MUL(x, 0x1p54));
+        ex = static_cast<int>((bits >> 52) & 0x7ff);
+        e = ex - 1023 - 54;
+    } else {
+        e = ex - 1023;
+    }
+    double m = MB_FROM_BITS((bits & 0x000fffffffffffffll) | 0x3ff0000000000000ll);
+    if (m > kSqrt2) {
+        m = MB_MUL(m, 0.5);
+        e += 1;
+    }
+    const double r = MB_SUB(m, 1.0);  // exact (Sterbenz)
+    const DD d = two_sum(m, 1.0);
+    const double zh = MB_DIV(r, d.hi);
+    double t = MB_FMA(-zh, d.hi, r);
+    t = MB_FMA(-zh, d.lo, t);
+    const DD z = fast_two_sum(zh, MB_DIV(t, d.hi));
+    const DD w = mul(z, z);
+    const double wh = w.hi;
+    // U = sum_{k=0}^{11} w^k / (2k + 5)
+    double U = 0x1.2f684bda12f68p-5;
+    U = MB_FMA(U, wh, 0x1.47ae147ae147bp-5);
+    U = MB_FMA(U, wh, 0x1.642c8590b2164p-5);
+    U = MB_FMA(U, wh, 0x1.8618618618618p-5);
+    U = MB_FMA(U, wh, 0x1.af286bca1af28p-5);
+    U = MB_FMA(U, wh, 0x1.e1e1e1e1e1e1ep-5);
+    U = MB_FMA(U, wh, 0x1.1111111111111p-4);
+    U = MB_FMA(U, wh, 0x1.3b13b13b13b14p-4);
+    U = MB_FMA(U, wh, 0x1.745d1745d1746p-4);
+    U = MB_FMA(U, wh, 0x1.c71c71c71c71cp-4);
+    U = MB_FMA(U, wh, 0x1.2492492492492p-3);
+    U = MB_FMA(U, wh, 0x1.999999999999ap-3);
+    const DD T = add(DD{kThirdHi, kThirdLo}, mul_d(w, U));  // 1/3 + w U
+    const DD S = add_d(mul(w, T), 1.0);                      // 1 + w T
+    DD lm = mul(z, S);
+    lm.hi = MB_MUL(lm.hi, 2.0);
+    lm.lo = MB_MUL(lm.lo, 2.0);
+    const double ed = static_cast<double>(e);
+    DD el = two_prod(ed, kLn2Hi);
+    el.lo = MB_FMA(ed, kLn2Lo, el.lo);
+    el = fast_two_sum(el.hi, el.lo);
+    const DD res = add(el, lm);
+    return MB_ADD(res.hi, res.lo);
+}
+
+// ---------------------------------------------------------------------------
+constexpr double kInvLn2 = 0x1.71547652b82fep+0;
+constexpr double kLn2Cw0 = 0x1.62e42fefa3800p-1;  // 42 significant bits: k * kLn2Cw0 is exact
+constexpr double kLn2Cw1 = 0x1.ef35793c76730p-45;
+constexpr double kLn2Cw2 = 0x1.f97b57a079a19p-103;
+
+MB_HD double scale2(double y, int k)
+{
+    if (k > 1023) {
+        y = MB_MUL(y, 0x1p1023);
+        k -= 1023;
+        if (k > 1023) k = 1023;
+    } else if (k < -1022) {
+        y = MB_MUL(y, 0x1p-600);
+        k += 600;
+        if (k < -1022) k = -1022;
+    }
+    return MB_MUL(y, MB_FROM_BITS(static_cast<long long>(k + 1023) << 52));
+}
+
+// Correctly rounded (see header) exponential for normal results; results in
+// the subnormal range are rounded twice.
+MB_HD double exp(double x)
+{
+    if (x != x) return x;
+    if (x > 709.782712893384) return MB_FROM_BITS(0x7ff0000000000000ll);
+    if (x < -745.2) return 0.0;
+    const double kd = MB_RINT(MB_MUL(x, kInvLn2));
+    const int k = static_cast<int>(kd);
+    const double r0 = MB_FMA(-kd, kLn2Cw0, x);  // exact
+    const DD p1 = two_prod(-kd, kLn2Cw1);
+    DD r = two_sum(r0, p1.hi);
+    r.lo = MB_ADD(r.lo, p1.lo);
+    r.lo = MB_FMA(-kd, kLn2Cw2, r.lo);
+    r = fast_two_sum(r.hi, r.lo);
+    const DD s{MB_MUL(r.hi, 0.0625), MB_MUL(r.lo, 0.0625)};
+    const double sh = s.hi;
+    // V = sum_{n=3}^{10} s^(n-3) / n!
+    double V = 0x1.27e4fb7789f5cp-22;
+    V = MB_FMA(V, sh, 0x1.71de3a556c734p-19);
+    V = MB_FMA(V, sh, 0x1.a01a01a01a01ap-16);
+    V = MB_FMA(V, sh, 0x1.a01a01a01a01ap-13);
+    V = MB_FMA(V, sh, 0x1.6c16c16c16c17p-10);
+    V = MB_FMA(V, sh, 0x1.1111111111111p-7);
+    V = MB_FMA(V, sh, 0x1.5555555555555p-5);
+    V = MB_FMA(V, sh, 0x1.5555555555555p-3);
+    const DD inner = add_d(mul_d(s, V), 0.5);
+    DD E = add(s, mul(mul(s, s), inner));  // expm1(s)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        E = add(DD{MB_MUL(E.hi, 2.0), MB_MUL(E.lo, 2.0)}, mul(E, E));  // expm1(2s)
+    }
+    const DD res = add_d(E, 1.0);
+    return scale2(MB_ADD(res.hi, res.lo), k);
+}
+
+// ---------------------------------------------------------------------------
+constexpr double kTwoOverPi = 0x1.45f306dc9c883p-1;
+constexpr double kPio2P1 = 0x1.921fb54400000p+0;  // 33 significant bits
+constexpr double kPio2P2 = 0x1.0b4611a600000p-34; // 33 significant bits
+constexpr double kPio2P3 = 0x1.3198a2e037073p-69;
+constexpr double kPio2P4 = 0x1.129024e088a68p-123;
+
+// sin and cos of a double, correctly rounded (see header) for |x| < 1e5;
+// larger arguments fall back to the device library.
+MB_HD void sincos(double x, double *sp, double *cp)
+{
+    if (!(x < 1e5 && x > -1e5)) {
+        MB_LIB_SINCOS(x, sp, cp);
+        return;
+    }
+    const double kd = MB_RINT(MB_MUL(x, kTwoOverPi));
+    const double t = MB_FMA(-kd, kPio2P1, x);  // exact
+    const DD p2 = two_prod(-kd, kPio2P2);
+    DD r = two_sum(t, p2.hi);
+    r.lo = MB_ADD(r.lo, p2.lo);
+    r.lo = MB_FMA(-kd, kPio2P3, r.lo);
+    r.lo = MB_FMA(-kd, kPio2P4, r.lo);
+    r = fast_two_sum(r.hi, r.lo);
+    const DD w = mul(r, r);
+    const double wh = w.hi;
+    // sin r = r (1 + w(-1/6 + w(1/120 + w(-1/5040 + w S4))))
+    double S4 = -0x1.761b41316381ap-75;
+    S4 = MB_FMA(S4, wh, 0x1.71b8ef6dcf572p-66);
+    S4 = MB_FMA(S4, wh, -0x1.2f49b46814157p-57);
+    S4 = MB_FMA(S4, wh, 0x1.952c77030ad4ap-49);
+    S4 = MB_FMA(S4, wh, -0x1.ae7f3e733b81fp-41);
+    S4 = MB_FMA(S4, wh, 0x1.6124613a86d09p-33);
+    S4 = MB_FMA(S4, wh, -0x1.ae64567f544e4p-26);
+    S4 = MB_FMA(S4, wh, 0x1.71de3a556c734p-19);
+    DD sp3 = add(DD{-0x1.a01a01a01a01ap-13, -0x1.a01a01a01a01ap-73}, mul_d(w, S4));
+    DD sp2 = add(DD{0x1.1111111111111p-7, 0x1.1111111111111p-63}, mul(w, sp3));
+    DD sp1 = add(DD{-0x1.5555555555555p-3, -0x1.5555555555555p-57}, mul(w, sp2));
+    const DD sn = mul(r, add_d(mul(w, sp1), 1.0));
+    // cos r = 1 + w(-1/2 + w(1/24 + w(-1/720 + w C4)))
+    double C4 = -0x1.0ce396db7f853p-70;
+    C4 = MB_FMA(C4, wh, 0x1.e542ba4020225p-62);
+    C4 = MB_FMA(C4, wh, -0x1.6827863b97d97p-53);
+    C4 = MB_FMA(C4, wh, 0x1.ae7f3e733b81fp-45);
+    C4 = MB_FMA(C4, wh, -0x1.93974a8c07c9dp-37);
+    C4 = MB_FMA(C4, wh, 0x1.1eed8eff8d898p-29);
+    C4 = MB_FMA(C4, wh, -0x1.27e4fb7789f5cp-22);
+    C4 = MB_FMA(C4, wh, 0x1.a01a01a01a01ap-16);
+    DD cp3 = add(DD{-0x1.6c16c16c16c17p-10, 0x1.f49f49f49f49fp-65}, mul_d(w, C4));
+    DD cp2 = add(DD{0x1.5555555555555p-5, 0x1.5555555555555p-59}, mul(w, cp3));
+    DD cp1 = add_d(mul(w, cp2), -0.5);
+    const DD cs = add_d(mul(w, cp1), 1.0);
+    const double s = MB_ADD(sn.hi, sn.lo);
+    const double c = MB_ADD(cs.hi, cs.lo);
+    const int q = static_cast<int>(static_cast<long long>(kd) & 3);
+    switch (q) {
+        case 0: *sp = s; *cp = c; break;
+        case 1: *sp = c; *cp = -s; break;
+        case 2: *sp = -s; *cp = -c; break;
+        default: *sp = -c; *cp = s; break;
+    }
+}
+
+MB_HD double cos(double x)
+{
+    double s, c;
+    sincos(x, &s, &c);
+    return c;
+}
+
+MB_HD double sin(double x)
+{
+    double s, c;
+    sincos(x, &s, &c);
+    return s;
+}
+
+}  // namespace dd
+}  // namespace mckl_b200

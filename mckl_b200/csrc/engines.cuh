@@ -273,48 +273,63 @@ struct ArsGen {
         __syncthreads();
     }
 
-    __device__ __forceinline__ static uint32_t lookup(const uint32_t *lane_tab, uint32_t byte)
+    // Shared-memory byte address of this lane's copy of Te0[x] is
+    // x * 128 + base, base = table + 4 * lane.  Bytes are pulled out and
+    // rotated with PRMT (one ALU op each); the address is one multiply-add.
+    __device__ __forceinline__ static uint32_t lds(uint32_t addr)
     {
-        return lane_tab[byte << 5];
+        uint32_t v;
+        asm("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(addr));
+        return v;
     }
 
-    __device__ __forceinline__ static uint32_t rot(uint32_t x, int r)
+    template <int B>
+    __device__ __forceinline__ static uint32_t te(uint32_t s, uint32_t base)
     {
-        return __funnelshift_l(x, x, r);
+        const uint32_t x = __byte_perm(s, 0u, 0x4440u | B);
+        uint32_t a;
+        asm("mad.lo.u32 %0, %1, 128, %2;" : "=r"(a) : "r"(x), "r"(base));
+        return lds(a);
     }
+
+    __device__ __forceinline__ static uint32_t rot8(uint32_t x) { return __byte_perm(x, x, 0x2103u); }
+    __device__ __forceinline__ static uint32_t rot16(uint32_t x) { return __byte_perm(x, x, 0x1032u); }
+    __device__ __forceinline__ static uint32_t rot24(uint32_t x) { return __byte_perm(x, x, 0x0321u); }
 
     __device__ __forceinline__ void block(const Ctr &c, uint32_t out[4]) const
     {
-        const uint32_t *lt = ars_smem_table() + (threadIdx.x & 31);
+        const uint32_t base =
+            static_cast<uint32_t>(__cvta_generic_to_shared(ars_smem_table())) + 4u * (threadIdx.x & 31u);
         uint32_t s0 = static_cast<uint32_t>(c.w[0]) ^ rk[0][0];
         uint32_t s1 = static_cast<uint32_t>(c.w[0] >> 32) ^ rk[0][1];
         uint32_t s2 = static_cast<uint32_t>(c.w[1]) ^ rk[0][2];
         uint32_t s3 = static_cast<uint32_t>(c.w[1] >> 32) ^ rk[0][3];
 #pragma unroll
         for (int r = 1; r <= 4; ++r) {
-            const uint32_t t0 = rk[r][0] ^ lookup(lt, s0 & 0xFF) ^ rot(lookup(lt, (s1 >> 8) & 0xFF), 8) ^
-                                rot(lookup(lt, (s2 >> 16) & 0xFF), 16) ^ rot(lookup(lt, s3 >> 24), 24);
-            const uint32_t t1 = rk[r][1] ^ lookup(lt, s1 & 0xFF) ^ rot(lookup(lt, (s2 >> 8) & 0xFF), 8) ^
-                                rot(lookup(lt, (s3 >> 16) & 0xFF), 16) ^ rot(lookup(lt, s0 >> 24), 24);
-            const uint32_t t2 = rk[r][2] ^ lookup(lt, s2 & 0xFF) ^ rot(lookup(lt, (s3 >> 8) & 0xFF), 8) ^
-                                rot(lookup(lt, (s0 >> 16) & 0xFF), 16) ^ rot(lookup(lt, s1 >> 24), 24);
-            const uint32_t t3 = rk[r][3] ^ lookup(lt, s3 & 0xFF) ^ rot(lookup(lt, (s0 >> 8) & 0xFF), 8) ^
-                                rot(lookup(lt, (s1 >> 16) & 0xFF), 16) ^ rot(lookup(lt, s2 >> 24), 24);
+            const uint32_t t0 = rk[r][0] ^ te<0>(s0, base) ^ rot8(te<1>(s1, base)) ^ rot16(te<2>(s2, base)) ^
+                                rot24(te<3>(s3, base));
+            const uint32_t t1 = rk[r][1] ^ te<0>(s1, base) ^ rot8(te<1>(s2, base)) ^ rot16(te<2>(s3, base)) ^
+                                rot24(te<3>(s0, base));
+            const uint32_t t2 = rk[r][2] ^ te<0>(s2, base) ^ rot8(te<1>(s3, base)) ^ rot16(te<2>(s0, base)) ^
+                                rot24(te<3>(s1, base));
+            const uint32_t t3 = rk[r][3] ^ te<0>(s3, base) ^ rot8(te<1>(s0, base)) ^ rot16(te<2>(s1, base)) ^
+                                rot24(te<3>(s2, base));
             s0 = t0;
             s1 = t1;
             s2 = t2;
             s3 = t3;
         }
-        // last round: S-box bytes (byte 1 of Te0) in ShiftRows order
-        auto sb = [lt](uint32_t byte) -> uint32_t { return (lookup(lt, byte) >> 8) & 0xFF; };
-        out[0] = rk[5][0] ^ sb(s0 & 0xFF) ^ (sb((s1 >> 8) & 0xFF) << 8) ^ (sb((s2 >> 16) & 0xFF) << 16) ^
-                 (sb(s3 >> 24) << 24);
-        out[1] = rk[5][1] ^ sb(s1 & 0xFF) ^ (sb((s2 >> 8) & 0xFF) << 8) ^ (sb((s3 >> 16) & 0xFF) << 16) ^
-                 (sb(s0 >> 24) << 24);
-        out[2] = rk[5][2] ^ sb(s2 & 0xFF) ^ (sb((s3 >> 8) & 0xFF) << 8) ^ (sb((s0 >> 16) & 0xFF) << 16) ^
-                 (sb(s1 >> 24) << 24);
-        out[3] = rk[5][3] ^ sb(s3 & 0xFF) ^ (sb((s0 >> 8) & 0xFF) << 8) ^ (sb((s1 >> 16) & 0xFF) << 16) ^
-                 (sb(s2 >> 24) << 24);
+        // last round: S-box byte = byte 1 of Te0, placed with PRMT in ShiftRows order
+        auto last = [base](uint32_t a, uint32_t b, uint32_t c2, uint32_t d) -> uint32_t {
+            const uint32_t x0 = te<0>(a, base), x1 = te<1>(b, base), x2 = te<2>(c2, base), x3 = te<3>(d, base);
+            const uint32_t lo = __byte_perm(x0, x1, 0x0051u);  // low bytes: x0.b1, x1.b1
+            const uint32_t hi = __byte_perm(x2, x3, 0x0051u);  // low bytes: x2.b1, x3.b1
+            return __byte_perm(lo, hi, 0x5410u);
+        };
+        out[0] = rk[5][0] ^ last(s0, s1, s2, s3);
+        out[1] = rk[5][1] ^ last(s1, s2, s3, s0);
+        out[2] = rk[5][2] ^ last(s2, s3, s0, s1);
+        out[3] = rk[5][3] ^ last(s3, s0, s1, s2);
     }
 };
 

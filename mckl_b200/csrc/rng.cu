@@ -127,6 +127,18 @@ struct WordView<uint64_t> {
     static constexpr int kPer32 = 2;
 };
 
+// Write block i into a shared staging buffer with 128-bit stores: consecutive
+// lanes then fill consecutive 16-byte slots (no bank conflicts).
+template <class G>
+__device__ __forceinline__ void stage_block(uint32_t *st32, int i, const uint32_t (&blk)[G::kWords])
+{
+    uint4 *dst = reinterpret_cast<uint4 *>(st32) + i * (G::kWords / 4);
+#pragma unroll
+    for (int q = 0; q < G::kWords / 4; ++q) {
+        dst[q] = make_uint4(blk[4 * q], blk[4 * q + 1], blk[4 * q + 2], blk[4 * q + 3]);
+    }
+}
+
 // Store N values of R starting at a pointer known to be 16-byte aligned.
 template <typename R, int N>
 __device__ __forceinline__ void store_aligned(R *p, const R (&v)[N])
@@ -224,8 +236,7 @@ __global__ void __launch_bounds__(256) k_staged(G g, Ctr base, uint32_t off, uin
             if (w0 + static_cast<uint64_t>(i) * WPB < total) {
                 uint32_t blk[G::kWords];
                 g.block(ctr_add(base, t * TB + i, G::kCtrWords), blk);
-#pragma unroll
-                for (int j = 0; j < G::kWords; ++j) st32[i * G::kWords + j] = blk[j];
+                stage_block<G>(st32, i, blk);
             }
         }
         __syncthreads();
@@ -285,8 +296,7 @@ __global__ void __launch_bounds__(256) k_normal(G g, Ctr base, uint32_t off, uin
         for (int i = threadIdx.x; i < nb; i += blockDim.x) {
             uint32_t blk[G::kWords];
             g.block(ctr_add(base, b0 + i, G::kCtrWords), blk);
-#pragma unroll
-            for (int j = 0; j < G::kWords; ++j) st32[i * G::kWords + j] = blk[j];
+            stage_block<G>(st32, i, blk);
         }
         __syncthreads();
         R *o = out + c * K;
@@ -373,7 +383,8 @@ static int launch_words(const G &g, const Ctr &B, uint32_t off, uint64_t n, type
     constexpr int WPB = G::kWords / WordView<W>::kPer32;
     constexpr int OPB = WPB / F::kIn;
     const bool aligned = (off == 0) && (reinterpret_cast<uintptr_t>(out) % 16 == 0);
-    const int ctas = std::is_same<G, ArsGen>::value ? 4 : 8;
+    // ARS: 32 KiB of table per CTA bounds residency at 6 CTAs per SM
+    const int ctas = std::is_same<G, ArsGen>::value ? 6 : 8;
     if (aligned) {
         const uint64_t nblk = n / OPB;
         if (nblk) {

@@ -8,6 +8,8 @@
 
 #include <cstdint>
 
+#include "crmath.cuh"
+
 namespace mckl_b200 {
 
 enum U01Variant { kCanonical = 0, kCC = 1, kCO = 2, kOC = 3, kOO = 4 };
@@ -84,10 +86,11 @@ struct RealOps<double> {
     __device__ static double mul(double a, double b) { return __dmul_rn(a, b); }
     __device__ static double add(double a, double b) { return __dadd_rn(a, b); }
     __device__ static double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
-    __device__ static double log(double a) { return ::log(a); }
+    __device__ static double log(double a) { return dd::log(a); }
+    __device__ static double exp(double a) { return dd::exp(a); }
     __device__ static double sqrt(double a) { return __dsqrt_rn(a); }
-    __device__ static void sincos(double a, double *s, double *c) { ::sincos(a, s, c); }
-    __device__ static double cos(double a) { return ::cos(a); }
+    __device__ static void sincos(double a, double *s, double *c) { dd::sincos(a, s, c); }
+    __device__ static double cos(double a) { return dd::cos(a); }
     template <typename W>
     __device__ static double u01(int v, W u) { return u01_f64(v, u); }
 };
@@ -99,6 +102,7 @@ struct RealOps<float> {
     __device__ static float add(float a, float b) { return __fadd_rn(a, b); }
     __device__ static float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
     __device__ static float log(float a) { return ::logf(a); }
+    __device__ static float exp(float a) { return ::expf(a); }
     __device__ static float sqrt(float a) { return __fsqrt_rn(a); }
     __device__ static void sincos(float a, float *s, float *c) { ::sincosf(a, s, c); }
     __device__ static float cos(float a) { return ::cosf(a); }

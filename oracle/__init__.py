@@ -111,6 +111,7 @@ class CPUPath:
             f("pf_ar1", [sz, sz, vp, d, d, d, d, vp, vp, i, d, vp, vp, vp, vp, vp, vp])
             f("kalman_ar1", [sz, vp, d, d, d, vp, vp])
             f("block", [ep, vp, vp])
+            f("math_f64", [i, sz, vp, vp, vp])
         else:
             f("pf_ar1", [sz, sz, vp, d, d, d, d, vp, vp, i, d, i, vp, vp, vp, vp, vp, vp, i])
             f("pf_ar1_batch", [sz, vp, sz, vp, vp, vp, vp, vp, vp, i, d, vp, i])
@@ -235,6 +236,13 @@ class CPUPath:
         y = np.zeros(T + 1)
         self._simulate_ar1(T, phi, sx, sy, sd0, _ptr(k), _ptr(x), _ptr(y))
         return x, y
+
+    def math_f64(self, fn: str, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros_like(x)
+        y2 = np.zeros_like(x) if fn == "sincos" else None
+        self._math_f64({"log": 0, "exp": 1, "sincos": 2}[fn], len(x), _ptr(x), _ptr(y), _ptr(y2))
+        return (y, y2) if fn == "sincos" else y
 
     def kalman_ar1(self, y, phi, sx, sy):
         y = np.ascontiguousarray(y, dtype=np.float64)

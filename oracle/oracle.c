@@ -719,6 +719,20 @@ int orc_pf_ar1(size_t N, size_t T, const double *y, double phi, double sx, doubl
     return 0;
 }
 
+/* glibc's double log (0), exp (1) and sin/cos (2): the functions the
+ * reference's transforms call (math/vmf.hpp:1008-1075). */
+int orc_math_f64(int fn, size_t n, const double *x, double *y, double *y2)
+{
+    for (size_t i = 0; i < n; ++i) {
+        switch (fn) {
+            case 0: y[i] = log(x[i]); break;
+            case 1: y[i] = exp(x[i]); break;
+            default: y[i] = sin(x[i]); if (y2) y2[i] = cos(x[i]); break;
+        }
+    }
+    return 0;
+}
+
 /* Kalman filter for the same model (not part of MCKL): exact log-likelihood
  * and its gradient with respect to (phi, sx, sy), prior x_0 ~ N(0, sd0^2) with
  * the stationary sd0 = sx / sqrt(1 - phi^2). Forward-mode derivatives. */
