@@ -117,6 +117,46 @@ int mckl_b200_exponential_f32(mckl_b200_engine_t *e, size_t n, float *r_dev, flo
 int mckl_b200_exponential_f64(mckl_b200_engine_t *e, size_t n, double *r_dev, double lambda,
     void *stream);
 
+/* ---- SMC: Weight (core/weight.hpp:64-227) --------------------------------
+ * W_dev: N normalised weights, updated in place; v_dev: N log-weight
+ * increments.  add_log: log W_i += v_i (Weight::add_log, :143-148); set_log:
+ * log W_i = v_i (Weight::set_log, :123-128); both then normalise exactly as
+ * Weight::normalize(true) does, including its sequential sums, so W matches
+ * the reference's bits up to the last-place rounding of exp/log.
+ * ess (host, nullable): Weight::ess().  log_nc (host, nullable): log of the
+ * normalising-constant ratio, log sum_i W_i^old exp(v_i) = max + log(sum).
+ * Synchronizes the stream when ess or log_nc is requested. */
+int mckl_b200_weight_set_log(size_t N, double *W_dev, const double *v_dev, double *ess, double *log_nc,
+    void *stream);
+int mckl_b200_weight_add_log(size_t N, double *W_dev, const double *v_dev, double *ess, double *log_nc_inc,
+    void *stream);
+
+/* ---- SMC: resampling (algorithm/resample.hpp) ---------------------------
+ * Uniform sequences of u01_rand_sorted / _stratified / _systematic
+ * (:216-268): kind 0 sorted, 1 stratified, 2 systematic; n doubles into u_dev. */
+int mckl_b200_u01_sequence(int kind, mckl_b200_engine_t *rng, size_t n, double *u_dev, void *stream);
+/* ResampleAlgorithm::operator()(N, M, rng, W, rep) (:514-566): scheme 0
+ * Multinomial, 1 Stratified, 2 Systematic, 3 Residual, 4 ResidualStratified,
+ * 5 ResidualSystematic (:569-593).  W_dev: N normalised weights; rep_dev: N
+ * replication counts (sum M).  The engine must have 32-bit results.
+ * Residual schemes synchronize (their number of uniforms depends on W). */
+int mckl_b200_resample(int scheme, size_t N, size_t M, mckl_b200_engine_t *rng, const double *W_dev,
+    uint64_t *rep_dev, void *stream);
+/* resample_trans_rep_index (:416-466): replication counts -> M parent
+ * indices; occupied slots keep their own particle.  Synchronizes. */
+int mckl_b200_rep_to_index(size_t N, size_t M, const uint64_t *rep_dev, uint64_t *idx_dev, void *stream);
+/* StateMatrix<ColMajor>::select with n == size() (core/state_matrix.hpp:239-253),
+ * in place: state_dev is N x dim column-major, row i <- row idx[i]. */
+int mckl_b200_select_f64(size_t N, size_t dim, const uint64_t *idx_dev, double *state_dev, void *stream);
+int mckl_b200_select_f32(size_t N, size_t dim, const uint64_t *idx_dev, float *state_dev, void *stream);
+
+/* Sequential left fold s_i = s_{i-1} + x_i (s_{-1} = s0) of n nonnegative
+ * doubles, bit-identical to the reference's `accw += w[i]` loops
+ * (algorithm/resample.hpp:395-403, core/weight.hpp:221).  prefix_dev
+ * (nullable) receives every s_i; *final_value (host) the last.  Synchronizes. */
+int mckl_b200_fold_f64(size_t n, const double *x_dev, double s0, double *prefix_dev, double *final_value,
+    void *stream);
+
 /* ---- diagnostics (no counterpart in the reference) ----------------------
  * The library's double-double log (fn 0), exp (fn 1) and sin/cos (fn 2; cos
  * into y2_dev when non-null) element-wise, for checking against a host libm. */

@@ -101,6 +101,104 @@ def math_f64(fn: str, x):
     return (y, y2) if code == 2 else y
 
 
+_weight_set_log = _bind("mckl_b200_weight_set_log", [_sz, _vp, _vp, _vp, _vp, _vp])
+_weight_add_log = _bind("mckl_b200_weight_add_log", [_sz, _vp, _vp, _vp, _vp, _vp])
+_fold_f64 = _bind("mckl_b200_fold_f64", [_sz, _vp, _d, _vp, _vp, _vp])
+
+
+_u01_sequence = _bind("mckl_b200_u01_sequence", [_i, _EP, _sz, _vp, _vp])
+_resample = _bind("mckl_b200_resample", [_i, _sz, _sz, _EP, _vp, _vp, _vp])
+_rep_to_index = _bind("mckl_b200_rep_to_index", [_sz, _sz, _vp, _vp, _vp])
+_select = {"f64": _bind("mckl_b200_select_f64", [_sz, _sz, _vp, _vp, _vp]),
+           "f32": _bind("mckl_b200_select_f32", [_sz, _sz, _vp, _vp, _vp])}
+
+Multinomial, Stratified, Systematic, Residual, ResidualStratified, ResidualSystematic = range(6)
+
+
+def u01_sequence(kind: int, rng: CounterEngine, n: int):
+    """kind 0 sorted, 1 stratified, 2 systematic (algorithm/resample.hpp:216-268)."""
+    torch = _torch()
+    u = torch.empty(max(n, 1), dtype=torch.float64, device="cuda")
+    _check(_u01_sequence(kind, ctypes.byref(rng.state), n, ctypes.c_void_p(u.data_ptr()), _stream_ptr()))
+    return u[:n]
+
+
+def resample(scheme: int, rng: CounterEngine, W, M=None):
+    """Replication counts: ResampleAlgorithm::operator()(N, M, rng, W, rep)."""
+    torch = _torch()
+    N = W.numel()
+    M = N if M is None else M
+    rep = torch.empty(N, dtype=torch.int64, device=W.device)
+    _check(_resample(scheme, N, M, ctypes.byref(rng.state), ctypes.c_void_p(W.data_ptr()),
+                     ctypes.c_void_p(rep.data_ptr()), _stream_ptr()))
+    return rep
+
+
+def rep_to_index(rep, M=None):
+    torch = _torch()
+    N = rep.numel()
+    M = int(rep.sum().item()) if M is None else M
+    idx = torch.empty(max(M, 1), dtype=torch.int64, device=rep.device)
+    _check(_rep_to_index(N, M, ctypes.c_void_p(rep.data_ptr()), ctypes.c_void_p(idx.data_ptr()), _stream_ptr()))
+    return idx[:M]
+
+
+def select(idx, state):
+    """In-place row selection of an N x dim column-major state (dim-major tensor [dim, N] or [N])."""
+    torch = _torch()
+    N = state.shape[-1]
+    dim = state.numel() // N
+    t = "f64" if state.dtype == torch.float64 else "f32"
+    _check(_select[t](N, dim, ctypes.c_void_p(idx.data_ptr()), ctypes.c_void_p(state.data_ptr()), _stream_ptr()))
+    return state
+
+
+def fold_f64(x, s0: float = 0.0, prefix=True):
+    """Exact emulation of the sequential left fold; returns (prefix tensor or None, final)."""
+    torch = _torch()
+    pre = torch.empty_like(x) if prefix else None
+    fin = ctypes.c_double()
+    _check(_fold_f64(x.numel(), ctypes.c_void_p(x.data_ptr()), s0,
+                     ctypes.c_void_p(pre.data_ptr()) if pre is not None else None, ctypes.byref(fin),
+                     _stream_ptr()))
+    return pre, fin.value
+
+
+class Weight:
+    """``mckl::Weight`` over a CUDA float64 tensor of normalised weights."""
+
+    def __init__(self, N: int, device="cuda"):
+        torch = _torch()
+        self.data = torch.full((N,), 1.0 / N, dtype=torch.float64, device=device)
+        self._ess = float(N)
+        self.log_nc = 0.0
+
+    def size(self) -> int:
+        return self.data.numel()
+
+    def ess(self) -> float:
+        return self._ess
+
+    def set_equal(self) -> None:
+        self.data.fill_(1.0 / self.size())
+        self._ess = float(self.size())
+
+    def _call(self, fn, v):
+        torch = _torch()
+        v = v.to(device=self.data.device, dtype=torch.float64).contiguous()
+        ess, lnc = ctypes.c_double(), ctypes.c_double()
+        _check(fn(self.size(), ctypes.c_void_p(self.data.data_ptr()), ctypes.c_void_p(v.data_ptr()),
+                  ctypes.byref(ess), ctypes.byref(lnc), _stream_ptr()))
+        self._ess = ess.value
+        self.log_nc = lnc.value
+
+    def set_log(self, v) -> None:
+        self._call(_weight_set_log, v)
+
+    def add_log(self, v) -> None:
+        self._call(_weight_add_log, v)
+
+
 def _check(rc: int) -> None:
     if rc != 0:
         raise MCKLB200Error(f"mckl_b200 error {rc}: {_lib.mckl_b200_last_error().decode()}")

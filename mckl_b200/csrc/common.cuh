@@ -131,6 +131,13 @@ inline void advance_calls(mckl_b200_engine_t &e, uint64_t q, uint64_t S)
     e.index = static_cast<uint32_t>(total % M);
 }
 
+// Round a byte count up to a multiple of 256 (every carved scratch region
+// starts on a 256-byte boundary).
+inline size_t align256(size_t n)
+{
+    return (n + 255) & ~static_cast<size_t>(255);
+}
+
 // Scratch device memory owned by the library, one growable buffer per device
 // and slot; reused across calls on the same stream order.
 void *scratch(int slot, size_t bytes, cudaStream_t stream);

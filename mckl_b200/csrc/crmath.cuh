@@ -23,7 +23,9 @@
 // series coefficients.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
+#include <cstring>
 
 // The same source compiles for the device (CUDA intrinsics, explicit
 // round-to-nearest) and for a host check against the C library (plain
@@ -31,8 +33,6 @@
 #if defined(__CUDACC__)
 #define MB_HD __host__ __device__ __forceinline__
 #else
-#include <cmath>
-#include <cstring>
 #define MB_HD inline
 #endif
 
@@ -159,10 +159,11 @@ MB_HD double log(double x)
     }
     const double r = MB_SUB(m, 1.0);  // exact (Sterbenz)
     const DD d = two_sum(m, 1.0);
-    const double zh = MB_DIV(r, d.hi);
+    const double inv = MB_DIV(1.0, d.hi);
+    const double zh = MB_MUL(r, inv);  // any rounding of zh is absorbed by the correction
     double t = MB_FMA(-zh, d.hi, r);
     t = MB_FMA(-zh, d.lo, t);
-    const DD z = fast_two_sum(zh, MB_DIV(t, d.hi));
+    const DD z = fast_two_sum(zh, MB_MUL(t, inv));
     const DD w = mul(z, z);
     const double wh = w.hi;
     // U = sum_{k=0}^{11} w^k / (2k + 5)

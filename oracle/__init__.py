@@ -112,6 +112,7 @@ class CPUPath:
             f("kalman_ar1", [sz, vp, d, d, d, vp, vp])
             f("block", [ep, vp, vp])
             f("math_f64", [i, sz, vp, vp, vp])
+            f("fold", [sz, vp, d, vp, vp])
         else:
             f("pf_ar1", [sz, sz, vp, d, d, d, d, vp, vp, i, d, i, vp, vp, vp, vp, vp, vp, i])
             f("pf_ar1_batch", [sz, vp, sz, vp, vp, vp, vp, vp, vp, i, d, vp, i])
@@ -243,6 +244,14 @@ class CPUPath:
         y2 = np.zeros_like(x) if fn == "sincos" else None
         self._math_f64({"log": 0, "exp": 1, "sincos": 2}[fn], len(x), _ptr(x), _ptr(y), _ptr(y2))
         return (y, y2) if fn == "sincos" else y
+
+    def fold(self, x, s0=0.0):
+        """Sequential left fold: (prefix values, final value)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        pre = np.zeros_like(x)
+        fin = np.zeros(1)
+        self._fold(len(x), _ptr(x), s0, _ptr(pre), _ptr(fin))
+        return pre, float(fin[0])
 
     def kalman_ar1(self, y, phi, sx, sy):
         y = np.ascontiguousarray(y, dtype=np.float64)

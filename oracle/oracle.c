@@ -719,6 +719,20 @@ int orc_pf_ar1(size_t N, size_t T, const double *y, double phi, double sx, doubl
     return 0;
 }
 
+/* Sequential left fold s_i = s_{i-1} + x_i from s_{-1} = s0 (the
+ * std::accumulate / `accw += w[i]` loops of core/weight.hpp:221 and
+ * algorithm/resample.hpp:395-403); prefix may be NULL. */
+int orc_fold(size_t n, const double *x, double s0, double *prefix, double *final_value)
+{
+    double s = s0;
+    for (size_t i = 0; i < n; ++i) {
+        s = s + x[i];
+        if (prefix) prefix[i] = s;
+    }
+    *final_value = s;
+    return 0;
+}
+
 /* glibc's double log (0), exp (1) and sin/cos (2): the functions the
  * reference's transforms call (math/vmf.hpp:1008-1075). */
 int orc_math_f64(int fn, size_t n, const double *x, double *y, double *y2)
