@@ -150,6 +150,22 @@ int mckl_b200_rep_to_index(size_t N, size_t M, const uint64_t *rep_dev, uint64_t
 int mckl_b200_select_f64(size_t N, size_t dim, const uint64_t *idx_dev, double *state_dev, void *stream);
 int mckl_b200_select_f32(size_t N, size_t dim, const uint64_t *idx_dev, float *state_dev, void *stream);
 
+/* ---- particle filters ----------------------------------------------------
+ * Plain FP64 bootstrap filter for x_0 ~ N(0, sd0^2), x_t = phi x_{t-1} +
+ * sx eps_t, y_t = x_t + sy eta_t, t = 1..T (y[0] unused; y is a HOST array of
+ * T + 1 values), in SMCSampler's step order (algorithm/smc.hpp:389-406):
+ * iteration 0 draws x_0; iteration t propagates with a Normal(0,1) batch from
+ * the model engine Philox4x32(mkey), weights with Weight::add_log, records
+ * the ESS and resamples with `scheme` (as in mckl_b200_resample) from the
+ * engine Philox4x32(rkey) when ESS < N * threshold.  *loglik (host) = sum over
+ * t of log sum_i W_{t-1,i} p(y_t | x_{t,i}).  ess_hist / resampled (host,
+ * T + 1 entries) and anc_dev ((T + 1) x N parent indices, rows written at
+ * resampling steps) are optional.  x_dev, W_dev (device, N) receive the final
+ * particles and weights.  Synchronizes once per step. */
+int mckl_b200_pf_ar1_plain_f64(size_t N, size_t T, const double *y, double phi, double sx, double sy, double sd0,
+    const uint32_t mkey[2], const uint32_t rkey[2], int scheme, double threshold, double *loglik,
+    double *ess_hist, uint8_t *resampled, uint64_t *anc_dev, double *x_dev, double *W_dev, void *stream);
+
 /* Sequential left fold s_i = s_{i-1} + x_i (s_{-1} = s0) of n nonnegative
  * doubles, bit-identical to the reference's `accw += w[i]` loops
  * (algorithm/resample.hpp:395-403, core/weight.hpp:221).  prefix_dev

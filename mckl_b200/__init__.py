@@ -153,6 +153,31 @@ def select(idx, state):
     return state
 
 
+_pf_plain = _bind("mckl_b200_pf_ar1_plain_f64", [_sz, _sz, _vp, _d, _d, _d, _d, _vp, _vp, _i, _d, _vp, _vp,
+                                                   _vp, _vp, _vp, _vp, _vp])
+
+
+def pf_ar1_plain(N, y, phi, sx, sy, sd0, mkey, rkey, scheme=2, threshold=0.5, record=False):
+    """Plain FP64 bootstrap particle filter (see mckl_b200_pf_ar1_plain_f64)."""
+    torch = _torch()
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    T = len(y) - 1
+    mk = (ctypes.c_uint32 * 2)(*[int(k) for k in mkey])
+    rk = (ctypes.c_uint32 * 2)(*[int(k) for k in rkey])
+    ll = ctypes.c_double()
+    ess = np.zeros(T + 1)
+    rs = np.zeros(T + 1, dtype=np.uint8)
+    anc = torch.zeros((T + 1, N), dtype=torch.int64, device="cuda") if record else None
+    x = torch.empty(N, dtype=torch.float64, device="cuda")
+    W = torch.empty(N, dtype=torch.float64, device="cuda")
+    _check(_pf_plain(N, T, y.ctypes.data_as(ctypes.c_void_p), phi, sx, sy, sd0, ctypes.cast(mk, _vp),
+                     ctypes.cast(rk, _vp), scheme, threshold, ctypes.byref(ll), ess.ctypes.data_as(ctypes.c_void_p),
+                     rs.ctypes.data_as(ctypes.c_void_p),
+                     ctypes.c_void_p(anc.data_ptr()) if anc is not None else None,
+                     ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(W.data_ptr()), _stream_ptr()))
+    return dict(loglik=ll.value, ess=ess, resampled=rs, anc=anc, x=x, W=W)
+
+
 def fold_f64(x, s0: float = 0.0, prefix=True):
     """Exact emulation of the sequential left fold; returns (prefix tensor or None, final)."""
     torch = _torch()

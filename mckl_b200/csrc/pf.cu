@@ -1,0 +1,146 @@
+// pf.cu -- the plain FP64 bootstrap particle filter for the AR(1) model
+//   x_0 ~ N(0, sd0^2),  x_t = phi x_{t-1} + sx eps_t,  y_t = x_t + sy eta_t
+// run in the reference's SMCSampler step order (algorithm/smc.hpp:389-406):
+// selection (propagate + weight) -> record ESS -> resample iff
+// ESS < N * threshold (ResampleEval, algorithm/resample.hpp:494-507) -> next.
+// Model noise comes from one sequential engine, as BackendSEQ's eval_range
+// does with rng_set[0] (smp/backend_seq.hpp:60-64); resampling uses the
+// particle's own engine (core/particle.hpp:364).  Every piece is the
+// bit-faithful kernel of its reference function; the loop itself runs on the
+// host and synchronizes once per step to read the ESS that decides the
+// resampling, as the reference's loop does.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "resample.cuh"
+#include "weight.cuh"
+
+namespace mckl_b200 {
+
+namespace {
+
+__global__ void k_fill(uint64_t n, double *a, double v)
+{
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        a[i] = v;
+    }
+}
+
+// x = phi x + sx eps; ll = lconst - (y - x)^2 hinv, each rounding as written
+__global__ void k_ar1_propagate(uint64_t n, double *x, const double *eps, double y, double phi, double sx,
+    double lconst, double hinv, double *ll)
+{
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const double a = __dmul_rn(phi, x[i]);
+        const double b = __dmul_rn(sx, eps[i]);
+        const double xn = __dadd_rn(a, b);
+        x[i] = xn;
+        const double r = __dsub_rn(y, xn);
+        ll[i] = __dsub_rn(lconst, __dmul_rn(__dmul_rn(r, r), hinv));
+    }
+}
+
+unsigned grid_of(uint64_t n)
+{
+    return static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 148 * 16)));
+}
+
+}  // namespace
+
+}  // namespace mckl_b200
+
+using namespace mckl_b200;
+
+extern "C" int mckl_b200_pf_ar1_plain_f64(size_t N, size_t T, const double *y, double phi, double sx, double sy,
+    double sd0, const uint32_t mkey[2], const uint32_t rkey[2], int scheme, double threshold, double *loglik,
+    double *ess_hist, uint8_t *resampled, uint64_t *anc_dev, double *x_dev, double *W_dev, void *stream)
+{
+    MB_CHECK_ARG(N > 0 && N < (1ull << 31), "N must be in [1, 2^31)");
+    MB_CHECK_ARG(y != nullptr && mkey != nullptr && rkey != nullptr && loglik != nullptr, "null argument");
+    MB_CHECK_ARG(x_dev != nullptr && W_dev != nullptr, "x_dev and W_dev are required");
+    MB_CHECK_ARG(scheme >= 0 && scheme <= 5, "scheme must be 0..5");
+    MB_CHECK_ARG(sy > 0 && sd0 > 0, "sy and sd0 must be positive");
+    cudaStream_t s = as_stream(stream);
+    // work buffers: eps, ll, rep, idx, result words
+    const size_t wsz = weight_scratch_bytes(N), rsz = resample_scratch_bytes(N, N), isz = rep_index_scratch_bytes(N, N);
+    const size_t buf = 4 * align256(N * sizeof(double)) + 512;
+    char *base = static_cast<char *>(scratch(5, buf + wsz + rsz + isz, s));
+    if (!base) {
+        set_error("particle filter scratch allocation failed");
+        return MCKL_B200_ERR_NOMEM;
+    }
+    double *eps = reinterpret_cast<double *>(base);
+    double *ll = reinterpret_cast<double *>(base + align256(N * 8));
+    uint64_t *rep = reinterpret_cast<uint64_t *>(base + 2 * align256(N * 8));
+    uint64_t *idx = reinterpret_cast<uint64_t *>(base + 3 * align256(N * 8));
+    double *wres = reinterpret_cast<double *>(base + 4 * align256(N * 8));
+    int *err = reinterpret_cast<int *>(base + 4 * align256(N * 8) + 256);
+    void *wscr = base + buf;
+    void *rscr = base + buf + wsz;
+    void *iscr = base + buf + wsz + rsz;
+
+    mckl_b200_engine_t em, er;
+    mckl_b200_engine_seed(&em, MCKL_B200_PHILOX4X32, 0);
+    mckl_b200_engine_seed(&er, MCKL_B200_PHILOX4X32, 0);
+    em.key[0] = mkey[0];
+    em.key[1] = mkey[1];
+    er.key[0] = rkey[0];
+    er.key[1] = rkey[1];
+
+    // constants of the observation density, computed as the reference does on the host
+    const double lconst = -std::log(sy) - 0.5 * std::log(2 * 3.14159265358979323846);
+    const double hinv = 0.5 / (sy * sy);
+    const double equal = 1.0 / static_cast<double>(N);
+    MB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+    k_fill<<<grid_of(N), 256, 0, s>>>(N, W_dev, equal);
+    MB_LAUNCH_CHECK();
+    double ess = static_cast<double>(N), ll_sum = 0.0;
+    for (size_t it = 0; it <= T; ++it) {
+        if (it == 0) {
+            int rc = mckl_b200_normal_f64(&em, N, x_dev, 0.0, sd0, stream);
+            if (rc != MCKL_B200_OK) return rc;
+        } else {
+            int rc = mckl_b200_normal_f64(&em, N, eps, 0.0, 1.0, stream);
+            if (rc != MCKL_B200_OK) return rc;
+            k_ar1_propagate<<<grid_of(N), 256, 0, s>>>(N, x_dev, eps, y[it], phi, sx, lconst, hinv, ll);
+            MB_LAUNCH_CHECK();
+            rc = weight_normalize_dev(N, W_dev, ll, 1, wscr, wres, s);
+            if (rc != MCKL_B200_OK) return rc;
+            double h[2];
+            MB_CUDA(cudaMemcpyAsync(h, wres, sizeof(h), cudaMemcpyDeviceToHost, s));
+            MB_CUDA(cudaStreamSynchronize(s));
+            ess = h[0];
+            ll_sum += h[1];
+        }
+        if (ess_hist) ess_hist[it] = ess;
+        if (resampled) resampled[it] = 0;
+        if (ess < static_cast<double>(N) * threshold) {
+            int rc = resample_dev(scheme, N, N, er, W_dev, rep, rscr, s);
+            if (rc != MCKL_B200_OK) return rc;
+            rc = rep_to_index_dev(N, N, rep, idx, iscr, err, s);
+            if (rc != MCKL_B200_OK) return rc;
+            if (anc_dev) {
+                MB_CUDA(cudaMemcpyAsync(anc_dev + it * N, idx, N * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+            }
+            rc = select_dev<double>(N, N, 1, idx, x_dev, x_dev, s);
+            if (rc != MCKL_B200_OK) return rc;
+            k_fill<<<grid_of(N), 256, 0, s>>>(N, W_dev, equal);
+            MB_LAUNCH_CHECK();
+            ess = static_cast<double>(N);
+            if (resampled) resampled[it] = 1;
+        }
+    }
+    int h = 0;
+    MB_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MB_CUDA(cudaStreamSynchronize(s));
+    if (h) {
+        set_error("particle filter: a look-back wait exceeded its limit");
+        return MCKL_B200_ERR_DEVICE;
+    }
+    *loglik = ll_sum;
+    return MCKL_B200_OK;
+}
