@@ -166,6 +166,23 @@ int mckl_b200_pf_ar1_plain_f64(size_t N, size_t T, const double *y, double phi, 
     const uint32_t mkey[2], const uint32_t rkey[2], int scheme, double threshold, double *loglik,
     double *ess_hist, uint8_t *resampled, uint64_t *anc_dev, double *x_dev, double *W_dev, void *stream);
 
+/* Weight::add_log without any device allocation (no counterpart in the
+ * reference).  Same contract and results as mckl_b200_weight_add_log, for
+ * host programs that cannot let a library call cudaMalloc: plugins whose host
+ * owns all device memory through its own pool or budget, code that must not
+ * synchronize the device the way an allocation can, or processes running at
+ * the memory limit.  Its working memory is a fixed 96 KiB array compiled into
+ * the library, held on every GPU that loads it until the process exits; N is
+ * limited to 4194304 (2^22) particles and larger N is rejected with
+ * MCKL_B200_ERR_ARG.  The first call on a device looks up that array's device
+ * address (cudaGetSymbolAddress) with the device current; make that first
+ * call before any stream capture.  All calls share the one array: calls that
+ * may run at the same time on the GPU (different streams, threads or graphs
+ * without an ordering between them) race and must be serialized by the
+ * caller.  Synchronizes when ess or log_nc_inc is requested. */
+int mckl_b200_weight_add_log_static(size_t N, double *W_dev, const double *v_dev, double *ess, double *log_nc_inc,
+    void *stream);
+
 /* Sequential left fold s_i = s_{i-1} + x_i (s_{-1} = s0) of n nonnegative
  * doubles, bit-identical to the reference's `accw += w[i]` loops
  * (algorithm/resample.hpp:395-403, core/weight.hpp:221).  prefix_dev
