@@ -183,6 +183,33 @@ int mckl_b200_pf_ar1_plain_f64(size_t N, size_t T, const double *y, double phi, 
 int mckl_b200_weight_add_log_static(size_t N, double *W_dev, const double *v_dev, double *ess, double *log_nc_inc,
     void *stream);
 
+/* Batched filters (the chosen form, no single counterpart in the reference:
+ * many SMCSampler runs at once).  F independent AR(1) filters, filter f with
+ * N[f] particles, parameters phi[f], sx[f], sy[f], stationary x_0 (sd0 =
+ * sx / sqrt(1 - phi^2)), observations y[f * (T + 1) + t] (HOST, t = 1..T), model
+ * stream Philox4x32(mkeys[2f], mkeys[2f+1]) and resampling stream
+ * Philox4x32(rkeys[2f], rkeys[2f+1]) consumed exactly as the plain filter
+ * consumes them, systematic resampling when ESS < N * threshold.  fp64 = 0:
+ * FP32 propagation and likelihoods, FP64 normaliser / log-likelihood / scan;
+ * fp64 = 1: all FP64; fp64 = 2: FP32 as for 0, plus an FP64 shadow of every
+ * particle driven by the same uniforms and by the FP32 run's resampling
+ * decisions and parent indices, whose log-likelihood
+ * (mckl_b200_batched_shadow) measures the FP32 arithmetic error alone.
+ * create uploads and allocates; run launches one
+ * persistent kernel (filters pulled from a queue, largest first); run_graph
+ * replays it from a CUDA graph captured on first use; results copies the F
+ * log-likelihood estimates and resampling counts to the host. */
+typedef struct mckl_b200_batched mckl_b200_batched_t;
+int mckl_b200_batched_create(mckl_b200_batched_t **out, size_t F, const size_t *N, size_t T, const double *y,
+    const double *phi, const double *sx, const double *sy, const uint32_t *mkeys, const uint32_t *rkeys,
+    double threshold, int fp64);
+int mckl_b200_batched_config(mckl_b200_batched_t *b, int threads, int ctas_per_sm);
+int mckl_b200_batched_run(mckl_b200_batched_t *b, void *stream);
+int mckl_b200_batched_run_graph(mckl_b200_batched_t *b, void *stream);
+int mckl_b200_batched_results(mckl_b200_batched_t *b, double *loglik, uint32_t *nresampled, void *stream);
+int mckl_b200_batched_shadow(mckl_b200_batched_t *b, double *loglik_fp64, void *stream);
+int mckl_b200_batched_destroy(mckl_b200_batched_t *b);
+
 /* Sequential left fold s_i = s_{i-1} + x_i (s_{-1} = s0) of n nonnegative
  * doubles, bit-identical to the reference's `accw += w[i]` loops
  * (algorithm/resample.hpp:395-403, core/weight.hpp:221).  prefix_dev

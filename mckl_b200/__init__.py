@@ -178,6 +178,99 @@ def pf_ar1_plain(N, y, phi, sx, sy, sd0, mkey, rkey, scheme=2, threshold=0.5, re
     return dict(loglik=ll.value, ess=ess, resampled=rs, anc=anc, x=x, W=W)
 
 
+_bt_create = _bind("mckl_b200_batched_create", [_vp, _sz, _vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _d, _i])
+_bt_config = _bind("mckl_b200_batched_config", [_vp, _i, _i])
+_bt_run = _bind("mckl_b200_batched_run", [_vp, _vp])
+_bt_run_graph = _bind("mckl_b200_batched_run_graph", [_vp, _vp])
+_bt_results = _bind("mckl_b200_batched_results", [_vp, _vp, _vp, _vp])
+_bt_destroy = _bind("mckl_b200_batched_destroy", [_vp])
+_bt_shadow = _bind("mckl_b200_batched_shadow", [_vp, _vp, _vp])
+
+
+def _arr(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+class BatchedFilters:
+    """Many independent AR(1) bootstrap filters in one persistent kernel
+    (mckl_b200_batched_*).  y: array [F, T + 1]; keys: arrays [F, 2]."""
+
+    def __init__(self, N, y, phi, sx, sy, mkeys, rkeys, threshold=0.5, fp64=False, shadow=False):
+        self.N = _arr(N, np.uint64)
+        self.y = _arr(y, np.float64)
+        self.F, T1 = self.y.shape
+        self.T = T1 - 1
+        self._keep = [self.N, self.y, _arr(phi, np.float64), _arr(sx, np.float64), _arr(sy, np.float64),
+                      _arr(mkeys, np.uint32), _arr(rkeys, np.uint32)]
+        h = ctypes.c_void_p()
+        ptrs = [a.ctypes.data_as(ctypes.c_void_p) for a in self._keep]
+        _check(_bt_create(ctypes.byref(h), self.F, ptrs[0], self.T, ptrs[1], ptrs[2], ptrs[3], ptrs[4], ptrs[5],
+                          ptrs[6], threshold, 2 if shadow else int(bool(fp64))))
+        self.h = h
+
+    def config(self, threads=256, ctas_per_sm=4):
+        _check(_bt_config(self.h, threads, ctas_per_sm))
+
+    def run(self, graph=False, stream=None):
+        _check((_bt_run_graph if graph else _bt_run)(self.h, _stream_ptr(stream)))
+
+    def results(self):
+        ll = np.zeros(self.F)
+        nr = np.zeros(self.F, dtype=np.uint32)
+        _check(_bt_results(self.h, ll.ctypes.data_as(ctypes.c_void_p), nr.ctypes.data_as(ctypes.c_void_p),
+                           _stream_ptr()))
+        return ll, nr
+
+    def shadow_loglik(self):
+        """FP64 log-likelihoods along the FP32 run's genealogy (shadow=True)."""
+        ll = np.zeros(self.F)
+        _check(_bt_shadow(self.h, ll.ctypes.data_as(ctypes.c_void_p), _stream_ptr()))
+        return ll
+
+    def close(self):
+        if getattr(self, "h", None):
+            _bt_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown: the library may already be gone
+            pass
+
+
+def batched_workload(F=4096, T=500, seed=1234, nmin=256, nmax=65536):
+    """The batched configuration: filter parameters from Philox4x32(seed)
+    canonical uniforms (phi ~ U[0.5, 0.99], sx ~ U[0.5, 2], sy ~ U[0.2, 1],
+    N = round(exp(U[ln nmin, ln nmax]))), observations of filter f simulated
+    with Philox4x32(key f, 10) (2T + 2 standard normals: x_0 = sd0 z_0,
+    x_t = phi x_{t-1} + sx z_t, y_t = x_t + sy z_{T+t}); model keys (f, 11),
+    resampling keys (f, 12)."""
+    torch = _torch()
+    g = Philox4x32()
+    g.key = (seed, 0)
+    u = u01_canonical_distribution(g, 4 * F, dtype="f64").cpu().numpy().reshape(F, 4)
+    phi = 0.5 + 0.49 * u[:, 0]
+    sx = 0.5 + 1.5 * u[:, 1]
+    sy = 0.2 + 0.8 * u[:, 2]
+    N = np.rint(np.exp(np.log(nmin) + (np.log(nmax) - np.log(nmin)) * u[:, 3])).astype(np.uint64)
+    z = torch.empty((F, 2 * T + 2), dtype=torch.float64, device="cuda")
+    for f in range(F):
+        gf = Philox4x32()
+        gf.key = (f, 10)
+        normal_distribution(gf, 2 * T + 2, z[f])
+    z = z.cpu().numpy()
+    sd0 = sx / np.sqrt(1 - phi * phi)
+    x = sd0 * z[:, 0]
+    y = np.zeros((F, T + 1))
+    for t in range(1, T + 1):
+        x = phi * x + sx * z[:, t]
+        y[:, t] = x + sy * z[:, T + t]
+    mkeys = np.stack([np.arange(F), np.full(F, 11)], axis=1).astype(np.uint32)
+    rkeys = np.stack([np.arange(F), np.full(F, 12)], axis=1).astype(np.uint32)
+    return dict(N=N, y=y, phi=phi, sx=sx, sy=sy, sd0=sd0, mkeys=mkeys, rkeys=rkeys)
+
+
 def fold_f64(x, s0: float = 0.0, prefix=True):
     """Exact emulation of the sequential left fold; returns (prefix tensor or None, final)."""
     torch = _torch()

@@ -1,0 +1,567 @@
+// pf_batched.cu -- the chosen form: many independent AR(1) bootstrap filters
+// with uneven particle counts in one persistent kernel.
+//
+// Each CTA pulls filters from a work queue (largest first) and runs all T
+// steps of a filter before taking the next.  Per step and filter:
+//   noise      Normal(0,1) from the filter's model stream, consumed exactly as
+//              normal_distribution does (random/normal_distribution.hpp:50-101:
+//              1024-value chunks, radius word i and angle word K/2 + i, odd n
+//              redrawn from two more words), so the plain FP64 path with the
+//              same keys sees the same uniforms;
+//   propagate  x = phi x + sx eps, log-likelihood, log-weight update: FP32;
+//   normalise  max, sum of exp and of exp^2 (ESS), log normaliser and the
+//              log-likelihood increment: FP64 accumulation;
+//   resample   systematic (algorithm/resample.hpp:258-268) when ESS < N/2,
+//              from the filter's resample stream (two words per event):
+//              FP64 inclusive scan of the weights, replication counts by the
+//              closed-form lower bound of the systematic grid, the reference's
+//              slot-preserving parent assignment (:416-466) by two CTA scans
+//              and a binary search per empty slot, then the particle gather.
+// Particle state (x, log-weights) lives in global memory, contiguous per
+// filter; only the filters in flight are touched, so it stays in L2.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "block_scan.cuh"
+#include "common.cuh"
+#include "pf_batched.cuh"
+
+namespace mckl_b200 {
+
+namespace {
+
+struct WordCache {
+    uint64_t blk;
+    uint32_t w[4];
+};
+
+__device__ __forceinline__ uint32_t word_at(const PhiloxGen &g, uint64_t w, WordCache &c)
+{
+    const uint64_t b = w >> 2;
+    if (b != c.blk) {
+        g.block(Ctr{{b + 1, 0, 0, 0}}, c.w);
+        c.blk = b;
+    }
+    return c.w[w & 3];
+}
+
+// U01OC<double> of a word, rounded to the propagation type
+template <typename R>
+__device__ __forceinline__ R u01oc(uint32_t w)
+{
+    return static_cast<R>(__dadd_rn(__dmul_rn(static_cast<double>(w), 0x1p-32), 0x1p-32));
+}
+
+template <typename R>
+struct Math;
+
+template <>
+struct Math<float> {
+    __device__ static float radius(float u) { return sqrtf(-2.0f * logf(u)); }
+    __device__ static void sincos2pi(float v, float *s, float *c) { sincospif(2.0f * v, s, c); }
+    __device__ static float cos2pi(float v) { return cospif(2.0f * v); }
+    __device__ static float exp(float a) { return expf(a); }
+};
+
+template <>
+struct Math<double> {
+    __device__ static double radius(double u) { return sqrt(-2.0 * log(u)); }
+    __device__ static void sincos2pi(double v, double *s, double *c) { sincospi(2.0 * v, s, c); }
+    __device__ static double cos2pi(double v) { return cospi(2.0 * v); }
+    __device__ static double exp(double a) { return ::exp(a); }
+};
+
+template <typename T>
+__device__ __forceinline__ T block_max(T v, T *sh)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    v = warp_max(v);
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        T w = lane < nw ? sh[lane] : -INFINITY;
+        w = warp_max(w);
+        if (lane == 0) sh[32] = w;
+    }
+    __syncthreads();
+    const T r = sh[32];
+    __syncthreads();
+    return r;
+}
+
+// SHADOW (with R = float): every particle also carries an FP64 copy that is
+// propagated with the same uniforms, weighted in FP64 and resampled with the
+// FP32 run's decisions and parent indices; its log-likelihood isolates the
+// FP32 arithmetic error from the Monte Carlo divergence a flipped ancestor
+// would otherwise start.
+template <typename R, int THREADS, bool SHADOW>
+__global__ void __launch_bounds__(THREADS) k_pf_batched(const BatchedFilter *filt, const int *order, int nf,
+    const double *y, int T, double threshold, R *xa, R *xb, R *lw, uint32_t *cnt, uint32_t *scanS,
+    uint32_t *epos, double *loglik, uint32_t *nresampled, int *queue, double *xsa, double *xsb, double *lws,
+    double *loglik_shadow)
+{
+    __shared__ double shd[33];
+    __shared__ R shr[33];
+    __shared__ unsigned long long shu[33];
+    __shared__ int sh_f;
+    // work arrays are indexed by each filter's particle offset
+    while (true) {
+        if (threadIdx.x == 0) {
+            const int k = atomicAdd(queue, 1);
+            sh_f = k < nf ? order[k] : -1;
+        }
+        __syncthreads();
+        const int f = sh_f;
+        __syncthreads();
+        if (f < 0) break;
+        const BatchedFilter F = filt[f];
+        const uint64_t N = F.n;
+        R *x = xa + F.off, *x2 = xb + F.off, *l = lw + F.off;
+        double *xs = SHADOW ? xsa + F.off : nullptr, *xs2 = SHADOW ? xsb + F.off : nullptr;
+        double *ls = SHADOW ? lws + F.off : nullptr;
+        const double phi_d = F.phi, sx_d = F.sx, sd0_d = F.sd0, lconst_d = F.lconst, hinv_d = F.hinv;
+        double Ls_prev = log(static_cast<double>(N)), lls_sum = 0.0;
+        uint32_t *ct = cnt + F.off, *sS = scanS + F.off, *ep = epos + F.off;
+        const PhiloxGen gm{F.mkey[0], F.mkey[1]}, gr{F.rkey[0], F.rkey[1]};
+        const uint64_t per_step = N + (N & 1) * 2;  // words of one normal_distribution(N) call
+        const uint64_t m = N / 1024, tail = N % 1024;
+        const R phi = static_cast<R>(F.phi), sx = static_cast<R>(F.sx), sd0 = static_cast<R>(F.sd0);
+        const R lconst = static_cast<R>(F.lconst), hinv = static_cast<R>(F.hinv);
+        double L_prev = log(static_cast<double>(N)), ll_sum = 0.0;
+        uint64_t events = 0;
+        for (int t = 0; t <= T; ++t) {
+            const uint64_t P = static_cast<uint64_t>(t) * per_step;
+            const R yt = static_cast<R>(y[static_cast<uint64_t>(f) * (T + 1) + t]);
+            // ---- noise, propagation, log-likelihood, log-weights; running max
+            R vmax = -INFINITY;
+            double vmax_s = -INFINITY;
+            const double yt_d = y[static_cast<uint64_t>(f) * (T + 1) + t];
+            const uint64_t pairs = m * 512 + tail / 2;
+            for (uint64_t q = threadIdx.x; q < pairs; q += THREADS) {
+                const uint64_t c = q / 512, i = q % 512;
+                const uint64_t nu = (c < m ? 1024 : tail) / 2;
+                const uint64_t base = P + c * 1024;
+                WordCache wc{~0ull, {0, 0, 0, 0}};
+                const uint32_t wrad = word_at(gm, base + i, wc);
+                const uint32_t wang = word_at(gm, base + nu + i, wc);
+                const R s = Math<R>::radius(u01oc<R>(wrad));
+                R sn, cs;
+                Math<R>::sincos2pi(u01oc<R>(wang), &sn, &cs);
+                const uint64_t p0 = c * 1024 + i, p1 = c * 1024 + nu + i;
+                if constexpr (SHADOW) {
+                    const double sd = Math<double>::radius(u01oc<double>(wrad));
+                    double snd, csd;
+                    Math<double>::sincos2pi(u01oc<double>(wang), &snd, &csd);
+                    const double e0 = sd * snd, e1 = sd * csd;
+                    double x0, x1;
+                    if (t == 0) {
+                        x0 = sd0_d * e0;
+                        x1 = sd0_d * e1;
+                        ls[p0] = 0;
+                        ls[p1] = 0;
+                    } else {
+                        x0 = phi_d * xs[p0] + sx_d * e0;
+                        x1 = phi_d * xs[p1] + sx_d * e1;
+                        const double r0 = yt_d - x0, r1 = yt_d - x1;
+                        const double l0 = ls[p0] + (lconst_d - r0 * r0 * hinv_d);
+                        const double l1 = ls[p1] + (lconst_d - r1 * r1 * hinv_d);
+                        ls[p0] = l0;
+                        ls[p1] = l1;
+                        vmax_s = fmax(vmax_s, fmax(l0, l1));
+                    }
+                    xs[p0] = x0;
+                    xs[p1] = x1;
+                }
+                const R e0 = s * sn, e1 = s * cs;
+                R x0, x1;
+                if (t == 0) {
+                    x0 = sd0 * e0;
+                    x1 = sd0 * e1;
+                    l[p0] = 0;
+                    l[p1] = 0;
+                } else {
+                    x0 = phi * x[p0] + sx * e0;
+                    x1 = phi * x[p1] + sx * e1;
+                }
+                x[p0] = x0;
+                x[p1] = x1;
+                if (t > 0) {
+                    const R r0 = yt - x0, r1 = yt - x1;
+                    const R l0 = l[p0] + (lconst - r0 * r0 * hinv);
+                    const R l1 = l[p1] + (lconst - r1 * r1 * hinv);
+                    l[p0] = l0;
+                    l[p1] = l1;
+                    vmax = fmax(vmax, fmax(l0, l1));
+                }
+            }
+            if ((N & 1) && threadIdx.x == THREADS - 1) {
+                // odd N: the last particle from the two words after the chunks
+                WordCache wc{~0ull, {0, 0, 0, 0}};
+                const R u = u01oc<R>(word_at(gm, P + N, wc));
+                const R v = u01oc<R>(word_at(gm, P + N + 1, wc));
+                const R e = Math<R>::radius(u) * Math<R>::cos2pi(v);
+                const uint64_t p = N - 1;
+                if constexpr (SHADOW) {
+                    WordCache wd{~0ull, {0, 0, 0, 0}};
+                    const double ud = u01oc<double>(word_at(gm, P + N, wd));
+                    const double vd = u01oc<double>(word_at(gm, P + N + 1, wd));
+                    const double ed = Math<double>::radius(ud) * Math<double>::cos2pi(vd);
+                    const double xn = t == 0 ? sd0_d * ed : phi_d * xs[p] + sx_d * ed;
+                    xs[p] = xn;
+                    if (t == 0) {
+                        ls[p] = 0;
+                    } else {
+                        const double r = yt_d - xn;
+                        const double ln = ls[p] + (lconst_d - r * r * hinv_d);
+                        ls[p] = ln;
+                        vmax_s = fmax(vmax_s, ln);
+                    }
+                }
+                const R xn = t == 0 ? sd0 * e : phi * x[p] + sx * e;
+                x[p] = xn;
+                if (t == 0) l[p] = 0;
+                if (t > 0) {
+                    const R r = yt - xn;
+                    const R ln = l[p] + (lconst - r * r * hinv);
+                    l[p] = ln;
+                    vmax = fmax(vmax, ln);
+                }
+            }
+            if (t == 0) {
+                __syncthreads();
+                continue;
+            }
+            const R lmax = block_max(vmax, shr);
+            // ---- FP64 normaliser: S = sum exp(l - lmax), Q = sum exp^2; the
+            // log-weights are shifted by lmax (kept <= 0) and the FP64 log
+            // normaliser of the shifted weights carried to the next step
+            double S = 0.0, Q = 0.0;
+            for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
+                const R lp = l[p] - lmax;
+                l[p] = lp;
+                const double e = static_cast<double>(Math<R>::exp(lp));
+                S += e;
+                Q += e * e;
+            }
+            S = block_sum(S, shd);
+            Q = block_sum(Q, shd);
+            const double L = static_cast<double>(lmax) + log(S);
+            ll_sum += L - L_prev;
+            L_prev = log(S);
+            if constexpr (SHADOW) {
+                const double lmax_s = block_max(vmax_s, shd);
+                double Ss = 0.0;
+                for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
+                    const double lp = ls[p] - lmax_s;
+                    ls[p] = lp;
+                    Ss += exp(lp);
+                }
+                Ss = block_sum(Ss, shd);
+                lls_sum += lmax_s + log(Ss) - Ls_prev;
+                Ls_prev = log(Ss);
+            }
+            const double ess = S * S / Q;
+            if (!(ess < static_cast<double>(N) * threshold)) continue;
+            // ---- systematic resampling
+            ++events;
+            uint32_t wr[2];
+            {
+                WordCache wc{~0ull, {0, 0, 0, 0}};
+                const uint64_t a = 2 * (events - 1);
+                wr[0] = word_at(gr, a, wc);
+                wr[1] = word_at(gr, a + 1, wc);
+            }
+            const double U = __dadd_rn(__dmul_rn(static_cast<double>(wr[0]), 0x1p-64),
+                __dmul_rn(static_cast<double>(wr[1]), 0x1p-32));
+            const double delta = 1.0 / static_cast<double>(N);
+            const double ud = U * delta;
+            const double invS = 1.0 / S;
+            // inclusive FP64 scan of normalised weights over tiles of THREADS;
+            // count_i = #{j : u_j < c_i}
+            double carry = 0.0;
+            for (uint64_t b = 0; b < N; b += THREADS) {
+                const uint64_t p = b + threadIdx.x;
+                const double w = p < N ? static_cast<double>(Math<R>::exp(l[p])) * invS : 0.0;
+                double tot;
+                const double c = carry + block_inclusive_sum(w, shd, &tot);
+                carry += tot;
+                if (p < N) {
+                    // lower bound of c on the grid fma(j, delta, ud), j in [0, N)
+                    double jf = ceil((c - ud) * static_cast<double>(N));
+                    long long j = jf < 0 ? 0 : (jf > static_cast<double>(N) ? static_cast<long long>(N) : static_cast<long long>(jf));
+                    while (j > 0 && fma(static_cast<double>(j - 1), delta, ud) >= c) --j;
+                    while (j < static_cast<long long>(N) && fma(static_cast<double>(j), delta, ud) < c) ++j;
+                    ct[p] = static_cast<uint32_t>(p + 1 == N ? N : j);
+                }
+            }
+            __syncthreads();
+            // replication counts -> empty slots and surplus copies (exclusive scans)
+            unsigned long long carry2 = 0;
+            for (uint64_t b = 0; b < N; b += THREADS) {
+                const uint64_t p = b + threadIdx.x;
+                uint32_t rep = 0;
+                if (p < N) rep = ct[p] - (p == 0 ? 0u : ct[p - 1]);
+                const unsigned long long v = p < N ? ((rep == 0 ? 1ull : 0ull) | (static_cast<unsigned long long>(rep > 0 ? rep - 1 : 0) << 32)) : 0ull;
+                unsigned long long tot;
+                const unsigned long long inc = block_inclusive_sum(v, shu, &tot);
+                const unsigned long long ex = carry2 + inc - v;
+                carry2 += tot;
+                if (p < N) {
+                    sS[p] = static_cast<uint32_t>(ex >> 32);
+                    if (rep == 0) ep[ex & 0xffffffffull] = static_cast<uint32_t>(p);
+                    x2[p] = x[p];  // occupied slots keep their particle
+                    if constexpr (SHADOW) xs2[p] = xs[p];
+                }
+            }
+            __syncthreads();
+            const uint64_t n_empty = carry2 & 0xffffffffull;
+            for (uint64_t k = threadIdx.x; k < n_empty; k += THREADS) {
+                uint64_t lo = 0, hi = N;  // last source with surplus prefix <= k
+                while (hi - lo > 1) {
+                    const uint64_t mid = (lo + hi) >> 1;
+                    if (sS[mid] <= k) {
+                        lo = mid;
+                    } else {
+                        hi = mid;
+                    }
+                }
+                x2[ep[k]] = x[lo];
+                if constexpr (SHADOW) xs2[ep[k]] = xs[lo];
+            }
+            __syncthreads();
+            for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
+                x[p] = x2[p];
+                l[p] = 0;
+                if constexpr (SHADOW) {
+                    xs[p] = xs2[p];
+                    ls[p] = 0;
+                }
+            }
+            L_prev = log(static_cast<double>(N));
+            Ls_prev = log(static_cast<double>(N));
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            loglik[f] = ll_sum;
+            nresampled[f] = static_cast<uint32_t>(events);
+            if constexpr (SHADOW) loglik_shadow[f] = lls_sum;
+        }
+        __syncthreads();
+    }
+}
+
+template <typename R, int THREADS, bool SHADOW>
+int launch_one(const BatchedArgs &a, const int *order, int nf, int *queue, int ctas, cudaStream_t s)
+{
+    k_pf_batched<R, THREADS, SHADOW><<<ctas, THREADS, 0, s>>>(a.filt, order, nf, a.y, a.T, a.threshold,
+        static_cast<R *>(a.xa), static_cast<R *>(a.xb), static_cast<R *>(a.lw), a.cnt, a.scanS, a.epos,
+        a.loglik, a.nresampled, queue, a.xsa, a.xsb, a.lws, a.loglik_shadow);
+    MB_LAUNCH_CHECK();
+    return MCKL_B200_OK;
+}
+
+template <typename R, bool SHADOW>
+int launch_threads(const BatchedArgs &a, const int *order, int nf, int threads, int *queue, int ctas, cudaStream_t s)
+{
+    switch (threads) {
+        case 128: return launch_one<R, 128, SHADOW>(a, order, nf, queue, ctas, s);
+        case 256: return launch_one<R, 256, SHADOW>(a, order, nf, queue, ctas, s);
+        case 512: return launch_one<R, 512, SHADOW>(a, order, nf, queue, ctas, s);
+        default: return launch_one<R, 1024, SHADOW>(a, order, nf, queue, ctas, s);
+    }
+}
+
+}  // namespace
+
+int pf_batched_launch(const BatchedArgs &a, const int *order, int nf, int threads, int ctas_per_sm, int *queue,
+    cudaStream_t s)
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int ctas = std::max(1, std::min(nf, sms * ctas_per_sm));
+    MB_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), s));
+    if (a.fp64) return launch_threads<double, false>(a, order, nf, threads, queue, ctas, s);
+    if (a.xsa) return launch_threads<float, true>(a, order, nf, threads, queue, ctas, s);
+    return launch_threads<float, false>(a, order, nf, threads, queue, ctas, s);
+}
+
+}  // namespace mckl_b200
+
+// ---------------------------------------------------------------------------
+// C ABI: a handle owns the uploaded filters, observations and work arrays, so
+// the launch itself (mckl_b200_batched_run) is a single capturable kernel.
+// ---------------------------------------------------------------------------
+struct mckl_b200_batched {
+    int F = 0, T = 0;
+    uint64_t total = 0;
+    double threshold = 0.5;
+    int fp64 = 0, threads = 256, ctas_per_sm = 4;
+    void *mem = nullptr;
+    mckl_b200::BatchedArgs a{};
+    int *order = nullptr, *queue = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t graph_stream = nullptr;
+};
+
+using namespace mckl_b200;
+
+extern "C" {
+
+int mckl_b200_batched_create(mckl_b200_batched_t **out, size_t F, const size_t *N, size_t T, const double *y,
+    const double *phi, const double *sx, const double *sy, const uint32_t *mkeys, const uint32_t *rkeys,
+    double threshold, int fp64)
+{
+    MB_CHECK_ARG(out != nullptr && F > 0 && T > 0, "bad arguments");
+    MB_CHECK_ARG(N && y && phi && sx && sy && mkeys && rkeys, "null argument");
+    std::vector<BatchedFilter> h(F);
+    uint64_t total = 0;
+    for (size_t f = 0; f < F; ++f) {
+        MB_CHECK_ARG(N[f] >= 1 && N[f] < (1ull << 31), "particle counts must be in [1, 2^31)");
+        MB_CHECK_ARG(sy[f] > 0 && phi[f] * phi[f] < 1, "need sy > 0 and |phi| < 1");
+        h[f].n = N[f];
+        h[f].off = total;
+        h[f].phi = phi[f];
+        h[f].sx = sx[f];
+        h[f].sd0 = sx[f] / std::sqrt(1 - phi[f] * phi[f]);
+        h[f].lconst = -std::log(sy[f]) - 0.5 * std::log(2 * 3.14159265358979323846);
+        h[f].hinv = 0.5 / (sy[f] * sy[f]);
+        h[f].mkey[0] = mkeys[2 * f];
+        h[f].mkey[1] = mkeys[2 * f + 1];
+        h[f].rkey[0] = rkeys[2 * f];
+        h[f].rkey[1] = rkeys[2 * f + 1];
+        total += (N[f] + 31) / 32 * 32;
+    }
+    // largest filters first (longest-processing-time order for the work queue)
+    std::vector<int> order(F);
+    for (size_t f = 0; f < F; ++f) order[f] = static_cast<int>(f);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return N[a] > N[b]; });
+    auto *b = new mckl_b200_batched;
+    b->F = static_cast<int>(F);
+    b->T = static_cast<int>(T);
+    b->total = total;
+    b->threshold = threshold;
+    const bool shadow = (fp64 == 2);
+    b->fp64 = (fp64 == 1) ? 1 : 0;
+    const size_t rs = b->fp64 ? 8 : 4;
+    const size_t bytes = align256(F * sizeof(BatchedFilter)) + align256(F * (T + 1) * 8) + 3 * align256(total * rs) +
+                         3 * align256(total * 4) + align256(F * 8) + align256(F * 4) + align256(F * 4) + 256 +
+                         (shadow ? 3 * align256(total * 8) + align256(F * 8) : 0);
+    if (cudaMalloc(&b->mem, bytes) != cudaSuccess) {
+        delete b;
+        set_error("batched filter allocation failed");
+        return MCKL_B200_ERR_NOMEM;
+    }
+    char *p = static_cast<char *>(b->mem);
+    auto take = [&p](size_t n) {
+        char *q = p;
+        p += align256(n);
+        return q;
+    };
+    b->a.filt = reinterpret_cast<BatchedFilter *>(take(F * sizeof(BatchedFilter)));
+    b->a.y = reinterpret_cast<double *>(take(F * (T + 1) * 8));
+    b->a.xa = take(total * rs);
+    b->a.xb = take(total * rs);
+    b->a.lw = take(total * rs);
+    b->a.cnt = reinterpret_cast<uint32_t *>(take(total * 4));
+    b->a.scanS = reinterpret_cast<uint32_t *>(take(total * 4));
+    b->a.epos = reinterpret_cast<uint32_t *>(take(total * 4));
+    b->a.loglik = reinterpret_cast<double *>(take(F * 8));
+    b->a.nresampled = reinterpret_cast<uint32_t *>(take(F * 4));
+    b->order = reinterpret_cast<int *>(take(F * 4));
+    b->queue = reinterpret_cast<int *>(take(256));
+    if (shadow) {
+        b->a.xsa = reinterpret_cast<double *>(take(total * 8));
+        b->a.xsb = reinterpret_cast<double *>(take(total * 8));
+        b->a.lws = reinterpret_cast<double *>(take(total * 8));
+        b->a.loglik_shadow = reinterpret_cast<double *>(take(F * 8));
+    }
+    b->a.T = static_cast<int>(T);
+    b->a.threshold = threshold;
+    b->a.fp64 = b->fp64;
+    MB_CUDA(cudaMemcpy(b->a.filt, h.data(), F * sizeof(BatchedFilter), cudaMemcpyHostToDevice));
+    MB_CUDA(cudaMemcpy(b->a.y, y, F * (T + 1) * 8, cudaMemcpyHostToDevice));
+    MB_CUDA(cudaMemcpy(b->order, order.data(), F * 4, cudaMemcpyHostToDevice));
+    *out = b;
+    return MCKL_B200_OK;
+}
+
+int mckl_b200_batched_config(mckl_b200_batched_t *b, int threads, int ctas_per_sm)
+{
+    MB_CHECK_ARG(b != nullptr, "null handle");
+    MB_CHECK_ARG(threads == 128 || threads == 256 || threads == 512 || threads == 1024, "threads: 128/256/512/1024");
+    MB_CHECK_ARG(ctas_per_sm >= 1 && ctas_per_sm <= 32, "ctas_per_sm in [1, 32]");
+    b->threads = threads;
+    b->ctas_per_sm = ctas_per_sm;
+    if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+    }
+    if (b->graph) {
+        cudaGraphDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    return MCKL_B200_OK;
+}
+
+int mckl_b200_batched_run(mckl_b200_batched_t *b, void *stream)
+{
+    MB_CHECK_ARG(b != nullptr, "null handle");
+    return pf_batched_launch(b->a, b->order, b->F, b->threads, b->ctas_per_sm, b->queue, as_stream(stream));
+}
+
+int mckl_b200_batched_run_graph(mckl_b200_batched_t *b, void *stream)
+{
+    MB_CHECK_ARG(b != nullptr, "null handle");
+    cudaStream_t s = as_stream(stream);
+    if (!b->exec) {
+        cudaStream_t cap;
+        MB_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        MB_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+        const int rc = pf_batched_launch(b->a, b->order, b->F, b->threads, b->ctas_per_sm, b->queue, cap);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(cap, &g);
+        cudaStreamDestroy(cap);
+        if (rc != MCKL_B200_OK) return rc;
+        MB_CUDA(ce);
+        b->graph = g;
+        MB_CUDA(cudaGraphInstantiate(&b->exec, g, 0));
+    }
+    MB_CUDA(cudaGraphLaunch(b->exec, s));
+    count_launch();
+    return MCKL_B200_OK;
+}
+
+int mckl_b200_batched_shadow(mckl_b200_batched_t *b, double *loglik_fp64, void *stream)
+{
+    MB_CHECK_ARG(b != nullptr && loglik_fp64 != nullptr, "null argument");
+    MB_CHECK_ARG(b->a.loglik_shadow != nullptr, "the handle was not created with fp64 = 2 (shadow)");
+    cudaStream_t s = as_stream(stream);
+    MB_CUDA(cudaMemcpyAsync(loglik_fp64, b->a.loglik_shadow, b->F * 8, cudaMemcpyDeviceToHost, s));
+    MB_CUDA(cudaStreamSynchronize(s));
+    return MCKL_B200_OK;
+}
+
+int mckl_b200_batched_results(mckl_b200_batched_t *b, double *loglik, uint32_t *nresampled, void *stream)
+{
+    MB_CHECK_ARG(b != nullptr, "null handle");
+    cudaStream_t s = as_stream(stream);
+    if (loglik) MB_CUDA(cudaMemcpyAsync(loglik, b->a.loglik, b->F * 8, cudaMemcpyDeviceToHost, s));
+    if (nresampled) MB_CUDA(cudaMemcpyAsync(nresampled, b->a.nresampled, b->F * 4, cudaMemcpyDeviceToHost, s));
+    MB_CUDA(cudaStreamSynchronize(s));
+    return MCKL_B200_OK;
+}
+
+int mckl_b200_batched_destroy(mckl_b200_batched_t *b)
+{
+    if (!b) return MCKL_B200_OK;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    if (b->mem) cudaFree(b->mem);
+    delete b;
+    return MCKL_B200_OK;
+}
+
+}  // extern "C"

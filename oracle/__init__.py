@@ -71,6 +71,8 @@ def build(ref: bool = False) -> None:
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
     if ref and os.path.isdir(os.path.join(REF_ROOT, "include", "mckl")):
         subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+        if os.path.exists(os.path.join(os.path.dirname(HERE), "mckl_b200", "libmckl_b200.so")):
+            subprocess.run(["make", "-s", "-C", HERE, "shim"], check=True)
 
 
 def _ptr(a):
