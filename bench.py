@@ -1,30 +1,56 @@
 """Benchmark of the B200 path (one JSON line on rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mckl_b200|reference]
-                    [--workload rng]
+                    [--workload smc|rng] [--filters F] [--obs T] [--parts all|timed]
 
-Workload `rng` (the RNG + distributions configuration): for each of
-Threefry4x64-20 and ARS-5, seeded 42, streams of 2^28 values as
-  raw u32 words, U01 (the reference's default U01Distribution = canonical) in
-  fp32 and fp64, Normal(0,1) in fp32 and fp64, Exponential(1) in fp32 and fp64.
-Every transform starts from a freshly seeded engine, exactly like one call of
-the reference's batch API.  `value` is the bytes written per second over the
-whole step (all ranks); outputs (1-2 GiB per call) are far larger than the
-126 MB L2, so no flush is needed between calls.  With N ranks each rank runs
-the same workload on its own counter range (ctr[1] = rank): weak scaling, no
-data-path collective.
+Workload `smc` (default, the batched SMC configuration): F = 4096 independent
+AR(1) bootstrap filters, phi ~ U[0.5, 0.99], sx ~ U[0.5, 2], sy ~ U[0.2, 1] and
+particle counts log-uniform in [256, 65536] (47.2 M particles in all), drawn
+from Philox4x32(1234); T = 500 observations per filter simulated from the
+filter's own seed; systematic resampling when ESS < N/2.  FP32 propagation
+and likelihoods, FP64 normaliser, log-likelihood and cumulative scan; one
+persistent launch, replayed from a CUDA graph, block shape chosen by the
+library's autotuner.  A step is one full pass (every filter, every
+observation); `value` is particle-steps per second over all ranks.  Inputs
+(parameters, observations) are resident in HBM when timing starts; a step
+streams ~1.1 GB of particle state per pass, far above the 126 MB L2, so no
+flush is needed.  Also measured in the same run (rank 0):
+  * `plain_gpu`: the plain FP64 filter (mckl_b200_pf_ar1_plain_f64, the
+    reference's step order) on 32 filters spread over the particle counts,
+    one after the other, extrapolated to all F filters by a least-squares
+    per-filter cost a + b N; `ratio_vs_plain` = per-GPU value / that rate;
+  * `accuracy`: per filter |logL_FP32 - logL_FP64| / |logL_FP64|, with
+    logL_FP64 the FP64 shadow run along the same genealogy (same counters,
+    same ancestors; target 1e-6), and the estimates' offset from the exact
+    Kalman log-likelihood;
+  * `rng`: the RNG + distributions configuration (see below), one step.
 
-`e2e` times the same calls through the same C ABI with page-locked HOST output
-buffers (the kernels write the words straight over the host link, as a drop-in
-for the reference's host-memory `rand(rng, n, r)` calls).
+Workload `rng`: for each of Threefry4x64-20 and ARS-5, seeded 42, 2^28 values
+per call: raw u32 words, U01 (the reference's default canonical U01) in fp32
+and fp64, Normal(0,1) fp32/fp64, Exponential(1) fp32/fp64, each call from a
+freshly seeded engine; `value` is bytes written per second (each output of
+1-2 GiB exceeds the L2), plus the Philox4x32 configuration (2^26 words, then
+2^24 U01OO doubles).
 
-`cpu_baseline` / `--impl reference` time the reference's own CPU code (MCKL
-compiled from its headers into oracle/_ref) with all host threads on a bounded
-sample of the same calls.
+With N ranks every rank runs the whole workload on its own keys or counter
+range (weak scaling, no data-path collective); time is the max over ranks.
+
+`e2e` is the same step through the public API with host buffers: every step
+copies the observations from page-locked host memory into the filters and
+reads the F log-likelihoods back (smc); the RNG calls write page-locked host
+buffers directly (rng).
+
+`cpu_baseline` and `--impl reference` run the reference's own CPU code (MCKL
+compiled from its headers into oracle/_ref) on all host threads, on a bounded
+sample of the same workload.
+
+`--parts timed` runs only the warm-up and the timed loop (for profilers).
 """
 from __future__ import annotations
 
 import argparse
+import ctypes
+import datetime
 import json
 import os
 import statistics
@@ -38,6 +64,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "batched SMC particle-steps/s vs plain GPU path at matched logL error; RNG GB/s"
 LOG2N = 28
+# MUFU (special-function unit) results per particle-step in the batched
+# kernel: lg2 for the Box-Muller radius, sin|cos for the angle (one pair per
+# two particles), ex2 for the weight; nominal 16 results / clock / SM.
+MUFU_PER_PS = 3.0
+MUFU_PER_CLK_SM = 16
 
 
 def measured_peaks():
@@ -45,8 +76,8 @@ def measured_peaks():
     if os.path.exists(p):
         with open(p) as f:
             d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
+        return float(d["hbm_gbs"]), float(d.get("sm_max_mhz", 1965.0)), "measured"
+    return 6650.0, 1965.0, "fallback"
 
 
 # ---------------------------------------------------------------------------
@@ -104,6 +135,145 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def max_over_ranks(v, world, dev):
+    if world == 1:
+        return v
+    import torch
+
+    t = torch.tensor([v], device=dev, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch
+
+        torch.distributed.barrier()
+
+
+def events():
+    import torch
+
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+# ---------------------------------------------------------------------------
+# SMC workload
+# ---------------------------------------------------------------------------
+def make_filters(mb, w, **kw):
+    return mb.BatchedFilters(w["N"], w["y"], w["phi"], w["sx"], w["sy"], w["mkeys"], w["rkeys"], **kw)
+
+
+def plain_sample(mb, w, T, nsample=32):
+    """Plain FP64 filter on `nsample` filters spread over N; fit t = a + b N."""
+    import numpy as np
+    import torch
+
+    F = len(w["N"])
+    order = np.argsort(w["N"], kind="stable")
+    idx = order[np.linspace(0, F - 1, min(nsample, F)).astype(int)]
+    ts, ns = [], []
+    for f in idx:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        mb.pf_ar1_plain(int(w["N"][f]), w["y"][f], w["phi"][f], w["sx"][f], w["sy"][f], w["sd0"][f],
+                        tuple(int(k) for k in w["mkeys"][f]), tuple(int(k) for k in w["rkeys"][f]),
+                        scheme=mb.Systematic)
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t0)
+        ns.append(float(w["N"][f]))
+    A = np.stack([np.ones(len(ns)), np.array(ns)], axis=1)
+    coef, *_ = np.linalg.lstsq(A, np.array(ts), rcond=None)
+    a, b = max(float(coef[0]), 0.0), max(float(coef[1]), 0.0)
+    total = float(np.sum(a + b * w["N"].astype(float)))
+    return {"particle_steps_per_s": float(w["N"].sum()) * T / total, "est_seconds_all_filters": total,
+            "fit_seconds_per_filter": {"a": a, "b_per_particle": b}, "measured_seconds": float(sum(ts)),
+            "sample": f"{len(idx)} filters spread over the particle counts, run one after the other; "
+                      "total extrapolated with t_f = a + b N_f (least squares)"}
+
+
+def bench_smc(args, rank, world, dev):
+    import numpy as np
+    import torch
+
+    import mckl_b200 as mb
+
+    T = args.obs
+    w = mb.batched_workload(F=args.filters, T=T, seed=1234 + 7919 * rank)
+    ps_per_step = float(w["N"].sum()) * T
+    b = make_filters(mb, w)
+    trials = b.autotune()
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        b.run(graph=True)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = ClockSampler(dev.index if dev.index is not None else 0)
+    clocks.start()
+    l0 = mb.launch_count()
+    t0, t1 = events()
+    t0.record(stream)
+    for _ in range(args.steps):
+        b.run(graph=True)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    launches = mb.launch_count() - l0
+    clk = clocks.stop()
+    elapsed = max_over_ranks(t0.elapsed_time(t1) / 1e3, world, dev)
+    value = world * ps_per_step * args.steps / elapsed
+    ll, nres = b.results()
+    out = dict(value=value, elapsed=elapsed, launches=launches, clocks=clk, ps_per_step=ps_per_step, w=w, ll=ll)
+    if args.parts == "timed":
+        b.close()
+        return out
+
+    # e2e: observations from page-locked host memory every step, results back
+    yh = torch.from_numpy(np.ascontiguousarray(w["y"])).pin_memory()
+    e2e_steps = max(1, min(args.steps, 3))
+    b.set_y(yh)
+    b.run(graph=True)
+    b.results()
+    barrier(world)
+    h0, h1 = events()
+    h0.record(stream)
+    for _ in range(e2e_steps):
+        b.set_y(yh)
+        b.run(graph=True)
+        b.results()
+    h1.record(stream)
+    torch.cuda.synchronize()
+    e2e_elapsed = max_over_ranks(h0.elapsed_time(h1) / 1e3, world, dev)
+    b.close()
+    out["e2e"] = {"value": world * ps_per_step * e2e_steps / e2e_elapsed, "unit": "particle-steps/s",
+                  "h2d_bytes_per_step": int(w["y"].nbytes), "d2h_bytes_per_step": int(len(w["N"]) * 12)}
+    extra = {"autotune": [{"threads": t, "ctas_per_sm": c, "ms": round(m, 3)} for (t, c, m) in trials],
+             "resampling_events_per_step": int(nres.sum())}
+    if rank == 0:
+        import oracle as O
+
+        bs = make_filters(mb, w, shadow=True)
+        best = min(trials, key=lambda r: r[2])
+        bs.config(best[0], best[1])
+        bs.run()
+        ll32, _ = bs.results()
+        ll64 = bs.shadow_loglik()
+        bs.close()
+        rel = np.abs(ll32 - ll64) / np.abs(ll64)
+        orc = O.CPUPath("oracle")
+        kf = np.array([orc.kalman_ar1(w["y"][f], w["phi"][f], w["sx"][f], w["sy"][f])[0] for f in range(len(w["N"]))])
+        extra["accuracy"] = {
+            "fp32_vs_fp64_same_genealogy_rel": {"max": float(rel.max()), "median": float(np.median(rel)),
+                                                "frac_le_1e-6": float(np.mean(rel <= 1e-6))},
+            "estimate_minus_kalman": {"mean": float(np.mean(ll - kf)), "std": float(np.std(ll - kf)),
+                                      "max_abs": float(np.max(np.abs(ll - kf)))},
+            "target": "|dlogL| <= 1e-6 |logL| against FP64 along the same genealogy"}
+        extra["plain_gpu"] = plain_sample(mb, w, T)
+        extra["ratio_vs_plain"] = value / world / extra["plain_gpu"]["particle_steps_per_s"]
+    out["extra"] = extra
+    return out
+
+
 # ---------------------------------------------------------------------------
 # RNG workload
 # ---------------------------------------------------------------------------
@@ -122,29 +292,26 @@ def rng_ops():
 
 
 def run_op(mb, call, g, n, buf32, buf64):
+    import torch
+
+    f32 = buf32.view(torch.float32)
     if call == "rand":
         mb.rand(g, n, buf32)
     elif call == "u01_f32":
-        mb.u01_canonical_distribution(g, n, _as_f32(buf32))
+        mb.u01_canonical_distribution(g, n, f32)
     elif call == "u01_f64":
         mb.u01_canonical_distribution(g, n, buf64)
     elif call == "normal_f32":
-        mb.normal_distribution(g, n, _as_f32(buf32))
+        mb.normal_distribution(g, n, f32)
     elif call == "normal_f64":
         mb.normal_distribution(g, n, buf64)
     elif call == "exp_f32":
-        mb.exponential_distribution(g, n, _as_f32(buf32))
+        mb.exponential_distribution(g, n, f32)
     elif call == "exp_f64":
         mb.exponential_distribution(g, n, buf64)
 
 
-def _as_f32(t):
-    import torch
-
-    return t.view(torch.float32)
-
-
-def bench_rng(args, rank, world, dev):
+def bench_rng(rank, world, dev, steps, warmup, e2e=True, clocks_on=True):
     import torch
 
     import mckl_b200 as mb
@@ -164,76 +331,42 @@ def bench_rng(args, rank, world, dev):
     def step(record=None):
         for (name, eng, call, bpv) in ops:
             if record is not None:
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
+                e0, e1 = events()
                 e0.record(stream)
             run_op(mb, call, fresh(eng), n, buf32, buf64)
             if record is not None:
                 e1.record(stream)
                 record.append((name, e0, e1, n * bpv))
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
-    clocks = ClockSampler(dev.index if dev.index is not None else 0)
-    clocks.start()
+    barrier(world)
+    clocks = ClockSampler(dev.index if dev.index is not None else 0) if clocks_on else None
+    if clocks:
+        clocks.start()
     launches0 = mb.launch_count()
     rec = []
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
+    t0, t1 = events()
     t0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         step(rec)
     t1.record(stream)
     torch.cuda.synchronize()
     launches = mb.launch_count() - launches0
-    clk = clocks.stop()
-    elapsed = t0.elapsed_time(t1) / 1e3
-    if world > 1:
-        t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        elapsed = float(t.item())
-        torch.distributed.barrier()
+    clk = clocks.stop() if clocks else None
+    elapsed = max_over_ranks(t0.elapsed_time(t1) / 1e3, world, dev)
     bytes_per_step = sum(n * bpv for (_, _, _, bpv) in ops)
-    value = world * bytes_per_step * args.steps / elapsed / 1e9
+    value = world * bytes_per_step * steps / elapsed / 1e9
     per_op = {}
     for (name, e0, e1, nbytes) in rec:
-        ms = e0.elapsed_time(e1)
         d = per_op.setdefault(name, {"ms": 0.0, "bytes": nbytes, "calls": 0})
-        d["ms"] += ms
+        d["ms"] += e0.elapsed_time(e1)
         d["calls"] += 1
     for d in per_op.values():
         d["ms"] /= d["calls"]
         d["GB_s"] = d["bytes"] / (d["ms"] / 1e3) / 1e9
-    dominant = max(per_op, key=lambda k: per_op[k]["ms"])
-
-    # e2e: same calls, page-locked host outputs written by the kernels directly
-    hbuf32 = torch.empty(n, dtype=torch.int32, pin_memory=True)
-    hbuf64 = torch.empty(n, dtype=torch.float64, pin_memory=True)
-    e2e_steps = max(1, min(2, args.steps))
-    for (name, eng, call, bpv) in ops[:1]:
-        run_op(mb, call, fresh(eng), n, hbuf32, hbuf64)
-    torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
-    h0 = torch.cuda.Event(enable_timing=True)
-    h1 = torch.cuda.Event(enable_timing=True)
-    h0.record(stream)
-    for _ in range(e2e_steps):
-        for (name, eng, call, bpv) in ops:
-            run_op(mb, call, fresh(eng), n, hbuf32, hbuf64)
-    h1.record(stream)
-    torch.cuda.synchronize()
-    e2e_elapsed = h0.elapsed_time(h1) / 1e3
-    if world > 1:
-        t = torch.tensor([e2e_elapsed], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_elapsed = float(t.item())
-    e2e_value = world * bytes_per_step * e2e_steps / e2e_elapsed / 1e9
-    # Philox4x32 configuration: 2^26 raw words, then 2^24 U01OO doubles from the same stream
-    g = mb.Philox4x32(42)
+    # Philox4x32 configuration: 2^26 raw words, then 2^24 U01OO doubles
     p32 = torch.empty(1 << 26, dtype=torch.int32, device=dev)
     p64 = torch.empty(1 << 24, dtype=torch.float64, device=dev)
     for _ in range(3):
@@ -241,119 +374,218 @@ def bench_rng(args, rank, world, dev):
     c1 = {}
     for name, fn, nbytes in (("rand_u32_2^26", lambda gg: mb.rand(gg, 1 << 26, p32), 4 << 26),
                              ("u01oo_f64_2^24", lambda gg: mb.u01_oo_distribution(gg, 1 << 24, p64), 8 << 24)):
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
+        a, bb = events()
         reps = 50
         a.record(stream)
         for _ in range(reps):
             fn(mb.Philox4x32(42))
-        b.record(stream)
+        bb.record(stream)
         torch.cuda.synchronize()
-        ms = a.elapsed_time(b) / reps
+        ms = a.elapsed_time(bb) / reps
         c1[name] = {"ms": round(ms, 4), "GB_s": round(nbytes / (ms / 1e3) / 1e9, 1)}
-    return dict(value=value, elapsed=elapsed, bytes_per_step=bytes_per_step, per_op=per_op, dominant=dominant,
-                philox_c1=c1,
-                clocks=clk, launches=launches, e2e=dict(value=e2e_value, unit="GB/s", h2d_bytes_per_step=0,
-                                                        d2h_bytes_per_step=bytes_per_step,
-                                                        note="kernels write page-locked host buffers directly"))
+    out = dict(value=value, elapsed=elapsed, bytes_per_step=bytes_per_step, per_op=per_op, clocks=clk,
+               launches=launches, philox_c1=c1)
+    if e2e:
+        hbuf32 = torch.empty(n, dtype=torch.int32, pin_memory=True)
+        hbuf64 = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        torch.cuda.synchronize()
+        barrier(world)
+        h0, h1 = events()
+        h0.record(stream)
+        for (name, eng, call, bpv) in ops:
+            run_op(mb, call, fresh(eng), n, hbuf32, hbuf64)
+        h1.record(stream)
+        torch.cuda.synchronize()
+        e2e_elapsed = max_over_ranks(h0.elapsed_time(h1) / 1e3, world, dev)
+        out["e2e"] = {"value": world * bytes_per_step / e2e_elapsed / 1e9, "unit": "GB/s",
+                      "h2d_bytes_per_step": 0, "d2h_bytes_per_step": bytes_per_step,
+                      "note": "kernels write page-locked host buffers directly"}
+    return out
 
 
-def cpu_rng_baseline(sample_log2=24, reps=1):
-    """The reference's CPU fills (oracle/_ref) on all host threads."""
-    import ctypes
-
+# ---------------------------------------------------------------------------
+# CPU: the reference's own code (oracle/_ref) on all host threads
+# ---------------------------------------------------------------------------
+def cpu_smc_reference(w, T, nfilters=64):
+    """One BackendSEQ SMCSampler per filter, OpenMP over a sample of filters."""
     import numpy as np
 
     import oracle as O
 
-    if O.have_ref():
-        cpu = O.CPUPath("ref")
-        kind = "reference"
-        threads = int(cpu._max_threads())
-    else:
+    if not O.have_ref():
         return None
+    cpu = O.CPUPath("ref")
+    threads = int(cpu._max_threads())
+    F = len(w["N"])
+    order = np.argsort(w["N"], kind="stable")
+    idx = order[np.linspace(0, F - 1, min(nfilters, F)).astype(int)]
+    N = np.ascontiguousarray(w["N"][idx], dtype=np.uint64)
+    y = np.ascontiguousarray(w["y"][idx])
+    phi, sx, sy = (np.ascontiguousarray(w[k][idx]) for k in ("phi", "sx", "sy"))
+    mk = np.ascontiguousarray(w["mkeys"][idx], dtype=np.uint32)
+    rk = np.ascontiguousarray(w["rkeys"][idx], dtype=np.uint32)
+    ll = np.zeros(len(idx))
+
+    def p(a):
+        return ctypes.c_void_p(a.ctypes.data)
+
+    t0 = time.perf_counter()
+    rc = cpu._pf_ar1_batch(len(idx), p(N), T, p(y), p(phi), p(sx), p(sy), p(mk), p(rk), 2, 0.5, p(ll), threads)
+    dt = time.perf_counter() - t0
+    if rc != 0:
+        raise RuntimeError("reference particle filter failed")
+    return dict(value=float(N.sum()) * T / dt, unit="particle-steps/s", cores=threads, kind="reference",
+                sample=f"{len(idx)} of the {F} filters spread over the particle counts ({int(N.sum())} particles, "
+                       f"T = {T}): MCKL SMCSampler + BackendSEQ per filter, OpenMP over filters; {dt:.1f} s")
+
+
+def cpu_rng_reference(sample_log2=24):
+    import numpy as np
+
+    import oracle as O
+
+    if not O.have_ref():
+        return None
+    cpu = O.CPUPath("ref")
+    threads = int(cpu._max_threads())
     n = 1 << sample_log2
     out = np.empty(n * 2, dtype=np.float64)
     total_bytes, total_s = 0, 0.0
-    for _ in range(reps):
-        for (name, eng, call, bpv) in rng_ops():
-            e = O.Engine.make(3 if eng == "Threefry4x64" else 5, key=(42,))
-            if call == "rand":
-                s = cpu._fill_u32_parallel(ctypes.byref(e), n, ctypes.c_void_p(out.ctypes.data), threads)
-            else:
-                dist = {"u01": 0, "normal": 5, "exp": 6}[call.split("_")[0]]
-                s = cpu._dist_parallel(ctypes.byref(e), dist, int(call.endswith("f64")), n,
-                                       ctypes.c_void_p(out.ctypes.data), threads)
-            total_bytes += n * bpv
-            total_s += s
-    return dict(value=total_bytes / total_s / 1e9, unit="GB/s", cores=threads, kind=kind,
+    for (name, eng, call, bpv) in rng_ops():
+        e = O.Engine.make(3 if eng == "Threefry4x64" else 5, key=(42,))
+        if call == "rand":
+            s = cpu._fill_u32_parallel(ctypes.byref(e), n, ctypes.c_void_p(out.ctypes.data), threads)
+        else:
+            dist = {"u01": 0, "normal": 5, "exp": 6}[call.split("_")[0]]
+            s = cpu._dist_parallel(ctypes.byref(e), dist, int(call.endswith("f64")), n,
+                                   ctypes.c_void_p(out.ctypes.data), threads)
+        total_bytes += n * bpv
+        total_s += s
+    return dict(value=total_bytes / total_s / 1e9, unit="GB/s", cores=threads, kind="reference",
                 sample=f"every call of the workload at 2^{sample_log2} values (1/{1 << (LOG2N - sample_log2)} "
                        f"of the full size), OpenMP over block-aligned counter ranges")
+
+
+def strip(d):
+    return {k: v for k, v in d.items() if k in ("value", "unit", "cores", "kind", "sample")}
 
 
 # ---------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mckl_b200", choices=["mckl_b200", "reference"])
-    ap.add_argument("--workload", default="rng", choices=["rng"])
+    ap.add_argument("--workload", default="smc", choices=["smc", "rng"])
+    ap.add_argument("--filters", type=int, default=4096)
+    ap.add_argument("--obs", type=int, default=500)
+    ap.add_argument("--parts", default="all", choices=["all", "timed"])
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    cfg = {"workload": "rng: Threefry4x64-20 and ARS-5 (seed 42), 2^28 values per call: raw u32, U01 "
-                       "(canonical) f32/f64, Normal(0,1) f32/f64, Exponential(1) f32/f64",
-           "values_per_call": 1 << LOG2N, "l2_flush": "none needed: every output (1-2 GiB) exceeds the 126 MB L2",
-           "parallelism": f"{world} independent rank(s), counter range per rank"}
+    smc = args.workload == "smc"
+    if smc:
+        cfg = {"workload": f"batched SMC: {args.filters} AR(1) bootstrap filters, N log-uniform in [256, 65536], "
+                           f"T = {args.obs}, systematic resampling at ESS < N/2, FP32 propagation + FP64 "
+                           "normaliser/scan/logL, one persistent launch replayed from a CUDA graph",
+               "filters": args.filters, "T": args.obs,
+               "parallelism": f"{world} rank(s), {args.filters} filters each (own seeds)",
+               "l2_flush": "none: one step streams ~1.1 GB of particle state, far above the 126 MB L2"}
+    else:
+        cfg = {"workload": "rng: Threefry4x64-20 and ARS-5 (seed 42), 2^28 values per call: raw u32, U01 "
+                           "(canonical) f32/f64, Normal(0,1) f32/f64, Exponential(1) f32/f64",
+               "values_per_call": 1 << LOG2N,
+               "l2_flush": "none needed: every output (1-2 GiB) exceeds the 126 MB L2",
+               "parallelism": f"{world} independent rank(s), counter range per rank"}
 
     if args.impl == "reference":
         if rank != 0:
             return
-        steps = []
+        if smc:
+            import mckl_b200 as mb  # generates the workload's parameters and observations only
+
+            w = mb.batched_workload(F=args.filters, T=args.obs, seed=1234)
+        vals, base = [], None
         for i in range(args.warmup + args.steps):
-            r = cpu_rng_baseline(sample_log2=24)
+            r = cpu_smc_reference(w, args.obs, 32) if smc else cpu_rng_reference()
             if r is None:
                 print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built on this host"}))
                 return
             if i >= args.warmup:
-                steps.append(r)
-        v = statistics.median(s["value"] for s in steps)
-        base = steps[0]
-        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": args.gpus,
+                vals.append(r["value"])
+                base = r
+        v = statistics.median(vals)
+        unit = "particle-steps/s" if smc else "GB/s"
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": unit, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "u32/f32/f64", "data": "synthetic", "config": cfg,
-                "cpu_baseline": {"value": v, "unit": "GB/s", "cores": base["cores"], "kind": base["kind"],
-                                 "sample": base["sample"]},
-                "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                "vs_baseline": None, "dtype": "f64" if smc else "u32/f32/f64", "data": "synthetic",
+                "config": cfg, "cpu_baseline": strip(dict(base, value=v)),
+                "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
 
     import torch
 
     if world > 1:
-        torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    res = bench_rng(args, rank, world, dev)
-    peak, peak_kind = measured_peaks()
-    dom = res["per_op"][res["dominant"]]
-    line = {
-        "metric": METRIC, "value": res["value"], "unit": "GB/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": res["elapsed"] / args.steps * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u32/f32/f64",
-        "data": "synthetic: counter-based streams, no input data", "config": cfg,
-        "roofline": {"bound": "hbm", "kernel": res["dominant"], "achieved": dom["GB_s"], "peak": peak,
-                     "peak_kind": f"{peak_kind} hbm_gbs", "unit": "GB/s", "frac": dom["GB_s"] / peak,
-                     "traffic": None},
-        "e2e": res["e2e"], "gpu_launches": res["launches"], "clocks": res["clocks"],
-        "per_op": {k: {"ms": round(v["ms"], 4), "GB_s": round(v["GB_s"], 1)} for k, v in res["per_op"].items()},
-        "philox4x32_config": res["philox_c1"],
-    }
-    if rank == 0 and world == 1:
-        cb = cpu_rng_baseline(sample_log2=24)
-        line["cpu_baseline"] = cb
+    hbm_peak, sm_max, peak_kind = measured_peaks()
+    if smc:
+        res = bench_smc(args, rank, world, dev)
+        sm_mhz = (res["clocks"] or {}).get("sm_mhz") or sm_max
+        achieved = res["value"] / world * MUFU_PER_PS / 1e9
+        peak = 148 * MUFU_PER_CLK_SM * sm_max / 1e3
+        line = {
+            "metric": METRIC, "value": res["value"], "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["elapsed"] / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic: AR(1) observations simulated from per-filter Philox4x32 seeds", "config": cfg,
+            "roofline": {"bound": "mufu", "kernel": "k_pf_batched<float>", "achieved": achieved, "peak": peak,
+                         "unit": "Gop/s", "frac": achieved / peak, "traffic": None,
+                         "peak_kind": "nominal: 16 MUFU results/clk/SM x 148 SMs x clocks.max.sm (the measured "
+                                      "peaks file has no MUFU figure)",
+                         "at_sampled_clock_frac": achieved / (148 * MUFU_PER_CLK_SM * sm_mhz / 1e3),
+                         "note": f"{MUFU_PER_PS:g} MUFU results per particle-step"},
+            "e2e": res.get("e2e"), "gpu_launches": res["launches"], "clocks": res["clocks"],
+        }
+        line.update(res.get("extra", {}))
+        if args.parts == "all":
+            rng = bench_rng(rank, world, dev, steps=1, warmup=1, e2e=False, clocks_on=False)
+            ph = rng["philox_c1"]["rand_u32_2^26"]["GB_s"]
+            line["rng"] = {"value_GB_s": rng["value"],
+                           "per_op": {k: {"ms": round(v["ms"], 4), "GB_s": round(v["GB_s"], 1)}
+                                      for k, v in rng["per_op"].items()},
+                           "philox4x32_config": rng["philox_c1"],
+                           "roofline": {"bound": "hbm", "kernel": "k_blocks<PhiloxGen> (2^26 raw words)",
+                                        "achieved": ph, "peak": hbm_peak, "unit": "GB/s",
+                                        "peak_kind": f"{peak_kind} hbm_gbs", "frac": ph / hbm_peak}}
+            if rank == 0 and world == 1:
+                cb = cpu_smc_reference(res["w"], args.obs, 64)
+                if cb:
+                    line["cpu_baseline"] = strip(cb)
+    else:
+        res = bench_rng(rank, world, dev, steps=args.steps, warmup=args.warmup)
+        dom_name = max(res["per_op"], key=lambda k: res["per_op"][k]["ms"])
+        dom = res["per_op"][dom_name]
+        line = {
+            "metric": METRIC, "value": res["value"], "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": res["elapsed"] / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32/f32/f64",
+            "data": "synthetic: counter-based streams, no input data", "config": cfg,
+            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": dom["GB_s"], "peak": hbm_peak,
+                         "peak_kind": f"{peak_kind} hbm_gbs", "unit": "GB/s", "frac": dom["GB_s"] / hbm_peak,
+                         "traffic": None},
+            "e2e": res["e2e"], "gpu_launches": res["launches"], "clocks": res["clocks"],
+            "per_op": {k: {"ms": round(v["ms"], 4), "GB_s": round(v["GB_s"], 1)} for k, v in res["per_op"].items()},
+            "philox4x32_config": res["philox_c1"],
+        }
+        if rank == 0 and world == 1:
+            cb = cpu_rng_reference()
+            if cb:
+                line["cpu_baseline"] = cb
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank == 0:

@@ -208,6 +208,15 @@ int mckl_b200_batched_run(mckl_b200_batched_t *b, void *stream);
 int mckl_b200_batched_run_graph(mckl_b200_batched_t *b, void *stream);
 int mckl_b200_batched_results(mckl_b200_batched_t *b, double *loglik, uint32_t *nresampled, void *stream);
 int mckl_b200_batched_shadow(mckl_b200_batched_t *b, double *loglik_fp64, void *stream);
+/* Replace the observations (HOST array of F x (T + 1), copied on `stream`). */
+/* Autotuner: times the candidate block shapes (threads per CTA x resident CTAs
+ * per SM, skipping shapes that do not fit) on this handle's own filters, one
+ * full run each, and configures the fastest.  The first `max_trials` trials
+ * are reported in threads[] / ctas_per_sm[] / ms[] (any may be NULL); the
+ * number of trials in *ntrials.  Synchronizes `stream`. */
+int mckl_b200_batched_autotune(mckl_b200_batched_t *b, int max_trials, int *threads, int *ctas_per_sm, float *ms,
+                               int *ntrials, void *stream);
+int mckl_b200_batched_set_y(mckl_b200_batched_t *b, const double *y, void *stream);
 int mckl_b200_batched_destroy(mckl_b200_batched_t *b);
 
 /* Sequential left fold s_i = s_{i-1} + x_i (s_{-1} = s0) of n nonnegative

@@ -185,6 +185,8 @@ _bt_run_graph = _bind("mckl_b200_batched_run_graph", [_vp, _vp])
 _bt_results = _bind("mckl_b200_batched_results", [_vp, _vp, _vp, _vp])
 _bt_destroy = _bind("mckl_b200_batched_destroy", [_vp])
 _bt_shadow = _bind("mckl_b200_batched_shadow", [_vp, _vp, _vp])
+_bt_set_y = _bind("mckl_b200_batched_set_y", [_vp, _vp, _vp])
+_bt_autotune = _bind("mckl_b200_batched_autotune", [_vp, _i, _vp, _vp, _vp, _vp, _vp])
 
 
 def _arr(a, dt):
@@ -220,6 +222,21 @@ class BatchedFilters:
         _check(_bt_results(self.h, ll.ctypes.data_as(ctypes.c_void_p), nr.ctypes.data_as(ctypes.c_void_p),
                            _stream_ptr()))
         return ll, nr
+
+    def autotune(self, stream=None):
+        """Time the candidate block shapes on these filters and keep the
+        fastest; returns [(threads, ctas_per_sm, ms), ...]."""
+        th = (ctypes.c_int * 16)()
+        cp = (ctypes.c_int * 16)()
+        ms = (ctypes.c_float * 16)()
+        n = ctypes.c_int()
+        _check(_bt_autotune(self.h, 16, th, cp, ms, ctypes.byref(n), _stream_ptr(stream)))
+        return [(th[k], cp[k], ms[k]) for k in range(min(n.value, 16))]
+
+    def set_y(self, y, stream=None):
+        """Copy new observations (host array [F, T + 1]; page-locked for an async copy)."""
+        ptr = y.data_ptr() if hasattr(y, "data_ptr") else np.ascontiguousarray(y, dtype=np.float64).ctypes.data
+        _check(_bt_set_y(self.h, ctypes.c_void_p(ptr), _stream_ptr(stream)))
 
     def shadow_loglik(self):
         """FP64 log-likelihoods along the FP32 run's genealogy (shadow=True)."""

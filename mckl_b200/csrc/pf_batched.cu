@@ -361,6 +361,24 @@ int launch_one(const BatchedArgs &a, const int *order, int nf, int *queue, int c
     return MCKL_B200_OK;
 }
 
+template <typename R, int THREADS, bool SHADOW>
+int occupancy_one(int *blocks)
+{
+    MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, k_pf_batched<R, THREADS, SHADOW>, THREADS, 0));
+    return MCKL_B200_OK;
+}
+
+template <typename R, bool SHADOW>
+int occupancy_threads(int threads, int *blocks)
+{
+    switch (threads) {
+        case 128: return occupancy_one<R, 128, SHADOW>(blocks);
+        case 256: return occupancy_one<R, 256, SHADOW>(blocks);
+        case 512: return occupancy_one<R, 512, SHADOW>(blocks);
+        default: return occupancy_one<R, 1024, SHADOW>(blocks);
+    }
+}
+
 template <typename R, bool SHADOW>
 int launch_threads(const BatchedArgs &a, const int *order, int nf, int threads, int *queue, int ctas, cudaStream_t s)
 {
@@ -373,6 +391,14 @@ int launch_threads(const BatchedArgs &a, const int *order, int nf, int threads, 
 }
 
 }  // namespace
+
+// resident CTAs per SM of the kernel variant the arguments select
+int pf_batched_occupancy(const BatchedArgs &a, int threads, int *blocks)
+{
+    if (a.fp64) return occupancy_threads<double, false>(threads, blocks);
+    if (a.xsa) return occupancy_threads<float, true>(threads, blocks);
+    return occupancy_threads<float, false>(threads, blocks);
+}
 
 int pf_batched_launch(const BatchedArgs &a, const int *order, int nf, int threads, int ctas_per_sm, int *queue,
     cudaStream_t s)
@@ -531,6 +557,65 @@ int mckl_b200_batched_run_graph(mckl_b200_batched_t *b, void *stream)
     }
     MB_CUDA(cudaGraphLaunch(b->exec, s));
     count_launch();
+    return MCKL_B200_OK;
+}
+
+int mckl_b200_batched_autotune(mckl_b200_batched_t *b, int max_trials, int *threads, int *ctas_per_sm,
+    float *ms, int *ntrials, void *stream)
+{
+    MB_CHECK_ARG(b != nullptr && max_trials >= 0, "bad arguments");
+    cudaStream_t s = as_stream(stream);
+    // candidate block shapes: 4 to 8 warps per scheduler in total, from many
+    // small CTAs (small filters keep every thread busy) to few large ones
+    // (fewer barriers per particle on the large filters)
+    static const int cand[][2] = {{128, 8}, {128, 12}, {256, 4}, {256, 6}, {512, 2}, {512, 3}, {1024, 1}, {1024, 2}};
+    int best = -1, n = 0;
+    float best_ms = 0.0f;
+    cudaEvent_t e0, e1;
+    MB_CUDA(cudaEventCreate(&e0));
+    MB_CUDA(cudaEventCreate(&e1));
+    // one untimed run first (module load, caches)
+    int rc = pf_batched_launch(b->a, b->order, b->F, 256, 4, b->queue, s);
+    for (int k = 0; rc == MCKL_B200_OK && k < static_cast<int>(sizeof(cand) / sizeof(cand[0])); ++k) {
+        int fit = 0;
+        rc = pf_batched_occupancy(b->a, cand[k][0], &fit);
+        if (rc != MCKL_B200_OK) break;
+        if (fit < cand[k][1]) continue;  // would not be resident at once
+        cudaEventRecord(e0, s);
+        rc = pf_batched_launch(b->a, b->order, b->F, cand[k][0], cand[k][1], b->queue, s);
+        cudaEventRecord(e1, s);
+        if (rc != MCKL_B200_OK) break;
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            rc = MCKL_B200_ERR_CUDA;
+            set_error("autotune: kernel failed");
+            break;
+        }
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, e0, e1);
+        if (n < max_trials) {
+            if (threads) threads[n] = cand[k][0];
+            if (ctas_per_sm) ctas_per_sm[n] = cand[k][1];
+            if (ms) ms[n] = t;
+        }
+        ++n;
+        if (best < 0 || t < best_ms) {
+            best = k;
+            best_ms = t;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (ntrials) *ntrials = n;
+    if (rc != MCKL_B200_OK) return rc;
+    MB_CHECK_ARG(best >= 0, "autotune: no candidate block shape fits");
+    return mckl_b200_batched_config(b, cand[best][0], cand[best][1]);
+}
+
+int mckl_b200_batched_set_y(mckl_b200_batched_t *b, const double *y, void *stream)
+{
+    MB_CHECK_ARG(b != nullptr && y != nullptr, "null argument");
+    MB_CUDA(cudaMemcpyAsync(b->a.y, y, static_cast<size_t>(b->F) * (b->T + 1) * 8, cudaMemcpyHostToDevice,
+        as_stream(stream)));
     return MCKL_B200_OK;
 }
 

@@ -86,3 +86,33 @@ def test_batched_fp32_accuracy_and_graph(env, small):
     b2.run()
     ll3, nr3 = b2.results()
     assert np.array_equal(ll3, ll) and np.array_equal(nr3, nr)
+
+
+def test_batched_autotune_and_set_y(env, small):
+    mb, _ = env
+    w = small
+    b = mb.BatchedFilters(w["N"], w["y"], w["phi"], w["sx"], w["sy"], w["mkeys"], w["rkeys"])
+    trials = b.autotune()
+    assert len(trials) >= 2 and all(ms > 0 for (_, _, ms) in trials)
+    best = min(trials, key=lambda r: r[2])
+    b.run(graph=True)
+    ll, nr = b.results()
+    ref = mb.BatchedFilters(w["N"], w["y"], w["phi"], w["sx"], w["sy"], w["mkeys"], w["rkeys"])
+    ref.config(best[0], best[1])
+    ref.run()
+    llr, nrr = ref.results()
+    assert np.array_equal(ll, llr) and np.array_equal(nr, nrr)
+    # new observations through set_y (page-locked source) == a handle built on them
+    y2 = np.ascontiguousarray(w["y"][::-1])
+    yh = torch.from_numpy(y2.copy()).pin_memory()
+    b.set_y(yh)
+    b.run(graph=True)
+    ll2, _ = b.results()
+    c = mb.BatchedFilters(w["N"], y2, w["phi"], w["sx"], w["sy"], w["mkeys"], w["rkeys"])
+    c.config(best[0], best[1])
+    c.run()
+    llc, _ = c.results()
+    assert np.array_equal(ll2, llc)
+    assert not np.array_equal(ll2, ll)
+    for h in (b, ref, c):
+        h.close()
