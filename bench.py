@@ -27,10 +27,11 @@ flush is needed.  Also measured in the same run (rank 0):
 
 Workload `rng`: for each of Threefry4x64-20 and ARS-5, seeded 42, 2^28 values
 per call: raw u32 words, U01 (the reference's default canonical U01) in fp32
-and fp64, Normal(0,1) fp32/fp64, Exponential(1) fp32/fp64, each call from a
-freshly seeded engine; `value` is bytes written per second (each output of
-1-2 GiB exceeds the L2), plus the Philox4x32 configuration (2^26 words, then
-2^24 U01OO doubles).
+and fp64, Normal(0,1) fp32/fp64, Exponential(1) fp32/fp64, Gamma fp32/fp64
+with shape ~ U[0.5, 10] per block of 4096 samples (block b an independent
+stream at counter (0, b)), each call from a freshly seeded engine; `value`
+is bytes written per second (each output of 1-2 GiB exceeds the L2), plus
+the Philox4x32 configuration (2^26 words, then 2^24 U01OO doubles).
 
 With N ranks every rank runs the whole workload on its own keys or counter
 range (weak scaling, no data-path collective); time is the max over ranks.
@@ -288,7 +289,25 @@ def rng_ops():
         ops.append((f"{eng}.normal_f64", eng, "normal_f64", 8))
         ops.append((f"{eng}.exponential_f32", eng, "exp_f32", 4))
         ops.append((f"{eng}.exponential_f64", eng, "exp_f64", 8))
+        ops.append((f"{eng}.gamma_f32", eng, "gamma_f32", 4))
+        ops.append((f"{eng}.gamma_f64", eng, "gamma_f64", 8))
     return ops
+
+
+GAMMA_BLOCK = 4096
+
+
+def gamma_shapes(nvalues):
+    """Shape per block of 4096 samples, U[0.5, 10] from Philox4x32(2024)."""
+    import numpy as np
+
+    import mckl_b200 as mb
+
+    nb = nvalues // GAMMA_BLOCK
+    g = mb.Philox4x32()
+    g.key = (2024, 0)
+    u = mb.u01_canonical_distribution(g, nb, dtype="f64").cpu().numpy()
+    return np.ascontiguousarray(0.5 + 9.5 * u)
 
 
 def run_op(mb, call, g, n, buf32, buf64):
@@ -309,6 +328,19 @@ def run_op(mb, call, g, n, buf32, buf64):
         mb.exponential_distribution(g, n, f32)
     elif call == "exp_f64":
         mb.exponential_distribution(g, n, buf64)
+    elif call == "gamma_f32":
+        mb.gamma_blocks(g, GAMMA_BLOCK, shapes(n), f32)
+    elif call == "gamma_f64":
+        mb.gamma_blocks(g, GAMMA_BLOCK, shapes(n), buf64)
+
+
+_SHAPES = {}
+
+
+def shapes(n):
+    if n not in _SHAPES:
+        _SHAPES[n] = gamma_shapes(n)
+    return _SHAPES[n]
 
 
 def bench_rng(rank, world, dev, steps, warmup, e2e=True, clocks_on=True):
@@ -453,7 +485,15 @@ def cpu_rng_reference(sample_log2=24):
     total_bytes, total_s = 0, 0.0
     for (name, eng, call, bpv) in rng_ops():
         e = O.Engine.make(3 if eng == "Threefry4x64" else 5, key=(42,))
-        if call == "rand":
+        if call.startswith("gamma"):
+            a = gamma_shapes(n)
+            t0 = time.perf_counter()
+            rc = cpu._gamma_blocks(ctypes.byref(e), int(call.endswith("f64")), len(a), GAMMA_BLOCK,
+                                   ctypes.c_void_p(a.ctypes.data), 1.0, ctypes.c_void_p(out.ctypes.data), threads)
+            s = time.perf_counter() - t0
+            if rc != 0:
+                raise RuntimeError("reference gamma failed")
+        elif call == "rand":
             s = cpu._fill_u32_parallel(ctypes.byref(e), n, ctypes.c_void_p(out.ctypes.data), threads)
         else:
             dist = {"u01": 0, "normal": 5, "exp": 6}[call.split("_")[0]]
@@ -495,7 +535,8 @@ def main():
                "l2_flush": "none: one step streams ~1.1 GB of particle state, far above the 126 MB L2"}
     else:
         cfg = {"workload": "rng: Threefry4x64-20 and ARS-5 (seed 42), 2^28 values per call: raw u32, U01 "
-                           "(canonical) f32/f64, Normal(0,1) f32/f64, Exponential(1) f32/f64",
+                           "(canonical) f32/f64, Normal(0,1) f32/f64, Exponential(1) f32/f64, Gamma f32/f64 with shape "
+                           "U[0.5, 10] per block of 4096 (block b: counter (0, b))",
                "values_per_call": 1 << LOG2N,
                "l2_flush": "none needed: every output (1-2 GiB) exceeds the 126 MB L2",
                "parallelism": f"{world} independent rank(s), counter range per rank"}
@@ -509,7 +550,7 @@ def main():
             w = mb.batched_workload(F=args.filters, T=args.obs, seed=1234)
         vals, base = [], None
         for i in range(args.warmup + args.steps):
-            r = cpu_smc_reference(w, args.obs, 32) if smc else cpu_rng_reference()
+            r = cpu_smc_reference(w, args.obs, 128) if smc else cpu_rng_reference()
             if r is None:
                 print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built on this host"}))
                 return
@@ -563,7 +604,7 @@ def main():
                                         "achieved": ph, "peak": hbm_peak, "unit": "GB/s",
                                         "peak_kind": f"{peak_kind} hbm_gbs", "frac": ph / hbm_peak}}
             if rank == 0 and world == 1:
-                cb = cpu_smc_reference(res["w"], args.obs, 64)
+                cb = cpu_smc_reference(res["w"], args.obs, 128)
                 if cb:
                     line["cpu_baseline"] = strip(cb)
     else:

@@ -117,6 +117,26 @@ int mckl_b200_exponential_f32(mckl_b200_engine_t *e, size_t n, float *r_dev, flo
 int mckl_b200_exponential_f64(mckl_b200_engine_t *e, size_t n, double *r_dev, double lambda,
     void *stream);
 
+/* Gamma(alpha, beta): gamma_distribution (random/gamma_distribution.hpp:57-302):
+ * chunks of 8192 bytes with the T / W / N / E algorithms chosen by alpha, the
+ * accepted values compacted in order, scalar fallback for the last few; the
+ * engine state after the call is the reference's.  One stream, so the chunks
+ * run in order on one CTA. */
+int mckl_b200_gamma_f32(mckl_b200_engine_t *e, size_t n, float *r_dev, float alpha, float beta, void *stream);
+int mckl_b200_gamma_f64(mckl_b200_engine_t *e, size_t n, double *r_dev, double alpha, double beta,
+    void *stream);
+
+/* Independent Gamma streams, one per block of `block` samples: block b draws
+ * gamma_distribution(rng_b, block, r + b * block, alpha_host[b], beta) with
+ * rng_b = *e with counter (0, b, 0, 0) and an empty buffer (the reference's
+ * rng.ctr() positioning, random/counter.hpp:129-133); *e is not changed.
+ * No counterpart entry point in the reference: it is the per-block loop a
+ * parallel caller writes around gamma_distribution. */
+int mckl_b200_gamma_blocks_f32(const mckl_b200_engine_t *e, size_t nblocks, size_t block, const double *alpha_host,
+    double beta, float *r_dev, void *stream);
+int mckl_b200_gamma_blocks_f64(const mckl_b200_engine_t *e, size_t nblocks, size_t block, const double *alpha_host,
+    double beta, double *r_dev, void *stream);
+
 /* ---- SMC: Weight (core/weight.hpp:64-227) --------------------------------
  * W_dev: N normalised weights, updated in place; v_dev: N log-weight
  * increments.  add_log: log W_i += v_i (Weight::add_log, :143-148); set_log:

@@ -85,6 +85,10 @@ _normal = {"f32": _bind("mckl_b200_normal_f32", [_EP, _sz, _vp, _f, _f, _vp]),
            "f64": _bind("mckl_b200_normal_f64", [_EP, _sz, _vp, _d, _d, _vp])}
 _exponential = {"f32": _bind("mckl_b200_exponential_f32", [_EP, _sz, _vp, _f, _vp]),
                 "f64": _bind("mckl_b200_exponential_f64", [_EP, _sz, _vp, _d, _vp])}
+_gamma = {"f32": _bind("mckl_b200_gamma_f32", [_EP, _sz, _vp, _f, _f, _vp]),
+          "f64": _bind("mckl_b200_gamma_f64", [_EP, _sz, _vp, _d, _d, _vp])}
+_gamma_blocks = {"f32": _bind("mckl_b200_gamma_blocks_f32", [_EP, _sz, _sz, _vp, _d, _vp, _vp]),
+                 "f64": _bind("mckl_b200_gamma_blocks_f64", [_EP, _sz, _sz, _vp, _d, _vp, _vp])}
 
 
 _math_f64 = _bind("mckl_b200_math_f64", [_i, _sz, _vp, _vp, _vp, _vp])
@@ -559,6 +563,26 @@ def exponential_distribution(rng, n, r=None, lam=1.0, dtype="f64", stream=None):
     r, t = _real_out(r, n, None if r is not None else dtype)
     ptr = _check_out(r, n, 8 if t == "f64" else 4)
     _check(_exponential[t](ctypes.byref(rng.state), n, ptr, lam, _stream_ptr(stream)))
+    return r
+
+
+def gamma_distribution(rng, n, r=None, alpha=1.0, beta=1.0, dtype="f64", stream=None):
+    """gamma_distribution(rng, n, r, alpha, beta): one stream, engine advanced."""
+    r, t = _real_out(r, n, None if r is not None else dtype)
+    ptr = _check_out(r, n, 8 if t == "f64" else 4)
+    _check(_gamma[t](ctypes.byref(rng.state), n, ptr, alpha, beta, _stream_ptr(stream)))
+    return r
+
+
+def gamma_blocks(rng, block, alpha, r=None, beta=1.0, dtype="f64", stream=None):
+    """Independent Gamma streams: block b = gamma_distribution of `block`
+    values with shape alpha[b] from rng positioned at counter (0, b)."""
+    alpha = np.ascontiguousarray(alpha, dtype=np.float64)
+    n = len(alpha) * block
+    r, t = _real_out(r, n, None if r is not None else dtype)
+    ptr = _check_out(r, n, 8 if t == "f64" else 4)
+    _check(_gamma_blocks[t](ctypes.byref(rng.state), len(alpha), block, alpha.ctypes.data_as(ctypes.c_void_p),
+                            beta, ptr, _stream_ptr(stream)))
     return r
 
 

@@ -1,0 +1,669 @@
+// gamma.cu -- Gamma(alpha, beta) transform of an engine stream, exactly as
+// the reference's gamma_distribution (random/gamma_distribution.hpp:57-302).
+//
+// The reference draws in chunks of K = 8192 / sizeof(R) values: one chunk
+// consumes a fixed block of engine words (2K uniforms for the T and W
+// algorithms, K uniforms + K normals for N, K uniforms for E), keeps the
+// accepted values in order, and repeats while more than K values are missing;
+// a last chunk covers the remainder and a scalar loop fills what that chunk
+// rejected.  Algorithm N also redraws, one scalar normal at a time, every
+// normal whose v = 1 + c w is not positive, so its word consumption depends on
+// the data.  How many chunks a call needs, and where each chunk's words start,
+// therefore depend on the previous chunks: the chunks of one stream run in
+// order.  A CTA owns one stream and processes each chunk with all its
+// threads: the chunk's words are staged in shared memory, every thread
+// transforms K / THREADS values, the N redraws are replayed by one thread in
+// index order, and the accepted values are compacted with a CTA-wide rank.
+// Independent streams (gamma_blocks: one stream per block of samples, each on
+// its own counter range) run one per CTA across the GPU.
+//
+// Math: double uses the correctly rounded double-double log/exp/sin/cos of
+// crmath.cuh; float evaluates log/exp/sin/cos in double and rounds once (a
+// correctly rounded float result except in double-rounding cases, about one
+// in 2^28).  Every multiply and add is an explicit _rn operation, fma only
+// where the reference calls fma.
+#include <algorithm>
+#include <cmath>
+#include <type_traits>
+#include <vector>
+
+#include "common.cuh"
+#include "dispatch.cuh"
+#include "transforms.cuh"
+
+namespace mckl_b200 {
+
+namespace {
+
+template <typename R>
+struct GOps;
+
+template <>
+struct GOps<double> {
+    static constexpr double kTwoPi = 0x1.921fb54442d18p+2;
+    static constexpr double k0331 = 0.0331;
+    __device__ static double mul(double a, double b) { return __dmul_rn(a, b); }
+    __device__ static double add(double a, double b) { return __dadd_rn(a, b); }
+    __device__ static double sub(double a, double b) { return __dsub_rn(a, b); }
+    __device__ static double div(double a, double b) { return __ddiv_rn(a, b); }
+    __device__ static double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+    __device__ static double log(double a) { return dd::log(a); }
+    __device__ static double exp(double a) { return dd::exp(a); }
+    __device__ static double sqrt(double a) { return __dsqrt_rn(a); }
+    __device__ static void sincos(double a, double *s, double *c) { dd::sincos(a, s, c); }
+};
+
+template <>
+struct GOps<float> {
+    static constexpr float kTwoPi = 0x1.921fb6p+2f;
+    static constexpr float k0331 = 0.0331f;
+    __device__ static float mul(float a, float b) { return __fmul_rn(a, b); }
+    __device__ static float add(float a, float b) { return __fadd_rn(a, b); }
+    __device__ static float sub(float a, float b) { return __fsub_rn(a, b); }
+    __device__ static float div(float a, float b) { return __fdiv_rn(a, b); }
+    __device__ static float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+    __device__ static float log(float a) { return __double2float_rn(::log(static_cast<double>(a))); }
+    __device__ static float exp(float a) { return __double2float_rn(::exp(static_cast<double>(a))); }
+    __device__ static float sqrt(float a) { return __fsqrt_rn(a); }
+    __device__ static void sincos(float a, float *s, float *c)
+    {
+        double sd, cd;
+        ::sincos(static_cast<double>(a), &sd, &cd);
+        *s = __double2float_rn(sd);
+        *c = __double2float_rn(cd);
+    }
+};
+
+// Per-stream constants of GammaDistributionConstant (:57-96), computed on the
+// host with the same libm as the reference.
+template <typename R>
+struct GammaParam {
+    R alpha, beta, d, c;
+    int alg;  // 0 T (alpha < 0.6), 1 W (alpha < 1), 2 N (alpha > 1), 3 E (alpha == 1)
+};
+
+template <typename R>
+GammaParam<R> gamma_param(R alpha, R beta)
+{
+    GammaParam<R> k{alpha, beta, 0, 0, 0};
+    if (alpha < static_cast<R>(0.6)) {
+        k.alg = 0;
+        k.d = 1 - alpha;
+        k.c = 1 / alpha;
+    } else if (alpha < 1) {
+        k.alg = 1;
+        const R t = alpha / (1 - alpha);
+        k.d = std::pow(alpha, t) * (1 - alpha);
+        k.c = 1 / alpha;
+    } else if (alpha > 1) {
+        k.alg = 2;
+        k.d = alpha - static_cast<R>(1) / 3;
+        k.c = 1 / (3 * std::sqrt(k.d));
+    } else {
+        k.alg = 3;
+    }
+    return k;
+}
+
+// CounterEngine state (counter, buffer index) of one stream inside a CTA,
+// advanced call by call exactly like the host bookkeeping (advance_call), so
+// the representation after the call matches the reference's.
+template <int CW>
+struct DevEngine {
+    Ctr ctr;
+    uint32_t idx;
+
+    __device__ void call(uint64_t n, uint32_t M)
+    {
+        const uint64_t id = idx < M ? idx : M;
+        const uint64_t remain = M - id;
+        if (n <= remain) {
+            idx = static_cast<uint32_t>(id + n);
+            return;
+        }
+        const uint64_t rem2 = n - remain, m = rem2 / M;
+        ctr = ctr_add(ctr, m + 1, CW);
+        idx = static_cast<uint32_t>(rem2 - m * M);
+    }
+
+    // u01_batch of n values from one-word conversions: n / K calls of K
+    // (each followed by an empty call) and one of n % K
+    __device__ void batch(uint64_t n, uint64_t K, uint32_t M)
+    {
+        for (uint64_t i = 0; i < n / K; ++i) {
+            call(K, M);
+            call(0, M);
+        }
+        call(n % K, M);
+    }
+};
+
+// Scalar word reader for one thread: word k of the stream (k counted from the
+// stream's first word at block B, offset off), one cached block.
+template <class G, typename W>
+struct ScalarWords {
+    static constexpr int WPB = G::kWords / WordView<W>::kPer32;
+    const G *g;
+    Ctr B;
+    uint32_t off;
+    uint64_t cached = ~0ull;
+    uint32_t blk[G::kWords];
+
+    __device__ W at(uint64_t k)
+    {
+        const uint64_t a = off + k, b = a / WPB;
+        if (b != cached) {
+            g->block(ctr_add(B, b, G::kCtrWords), blk);
+            cached = b;
+        }
+        const int j = static_cast<int>(a % WPB);
+        W r = 0;
+#pragma unroll
+        for (int q = 0; q < WPB; ++q)
+            if (q == j) r = WordView<W>::get(blk, q);
+        return r;
+    }
+};
+
+// CTA-wide rank of a predicate in thread order: returns the number of
+// threads below this one with f set; *total gets the CTA count.  `sh` holds
+// one word per warp plus one.
+template <int THREADS>
+__device__ __forceinline__ uint32_t block_rank(bool f, uint32_t *sh, uint32_t *total)
+{
+    constexpr int NW = THREADS / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t b = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) sh[warp] = __popc(b);
+    __syncthreads();
+    uint32_t before = 0, tot = 0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+        const uint32_t c = sh[w];
+        before += (w < warp) ? c : 0u;
+        tot += c;
+    }
+    __syncthreads();
+    *total = tot;
+    return before + __popc(b & ((1u << lane) - 1u));
+}
+
+// Scalar normal with the cached second variate (random/normal_distribution.hpp:136-153).
+template <typename R>
+struct ScalarNormal {
+    R saved = 0;
+    bool has = false;
+
+    template <class SW>
+    __device__ R operator()(SW &sw, uint64_t &k)
+    {
+        using O = GOps<R>;
+        R z;
+        if (has) {
+            z = saved;
+            has = false;
+        } else {
+            const R a = RealOps<R>::u01(kOC, sw.at(k++));
+            const R u1 = O::sqrt(O::mul(static_cast<R>(-2), O::log(a)));
+            const R b = RealOps<R>::u01(kOC, sw.at(k++));
+            const R u2 = O::mul(O::kTwoPi, b);
+            R sn, cs;
+            O::sincos(u2, &sn, &cs);
+            z = O::mul(u1, cs);
+            saved = O::mul(u1, sn);
+            has = true;
+        }
+        return O::add(static_cast<R>(0), O::mul(static_cast<R>(1), z));
+    }
+};
+
+// GammaDistribution::generate_{t,w,n,e} (:350-459), the scalar fallback.
+template <typename R, class SW>
+__device__ R gamma_scalar(const GammaParam<R> &k, SW &sw, uint64_t &pos)
+{
+    using O = GOps<R>;
+    const R d = k.d, c = k.c;
+    R r = 0;
+    switch (k.alg) {
+        case 0:
+            for (;;) {
+                R u = O::sub(static_cast<R>(1), RealOps<R>::u01(kOO, sw.at(pos++)));
+                R e = -O::log(RealOps<R>::u01(kOO, sw.at(pos++)));
+                if (u > d) {
+                    u = -O::log(O::mul(c, O::sub(static_cast<R>(1), u)));
+                    e = O::add(e, u);
+                    u = O::add(d, O::mul(k.alpha, u));
+                }
+                r = O::exp(O::mul(c, O::log(u)));
+                if (fabs(r) < e) break;
+            }
+            break;
+        case 1: {
+            R u, e;
+            do {
+                u = -O::log(RealOps<R>::u01(kOO, sw.at(pos++)));
+                e = -O::log(RealOps<R>::u01(kOO, sw.at(pos++)));
+                r = O::exp(O::mul(c, O::log(u)));
+            } while (O::add(u, e) < O::add(d, r));
+            break;
+        }
+        case 2: {
+            ScalarNormal<R> rn;
+            for (;;) {
+                const R u = RealOps<R>::u01(kOO, sw.at(pos++));
+                R w, v;
+                do {
+                    w = rn(sw, pos);
+                    v = O::add(static_cast<R>(1), O::mul(c, w));
+                } while (v <= 0);
+                v = O::mul(O::mul(v, v), v);
+                const R w2 = O::mul(w, w);
+                R e = O::sub(static_cast<R>(1), O::mul(O::mul(O::k0331, w2), w2));
+                if (u < e) {
+                    r = O::mul(d, v);
+                    break;
+                }
+                e = O::add(O::div(w2, static_cast<R>(2)),
+                    O::mul(d, O::add(O::sub(static_cast<R>(1), v), O::log(v))));
+                if (O::log(u) < e) {
+                    r = O::mul(d, v);
+                    break;
+                }
+            }
+            break;
+        }
+        default:
+            r = -O::log(RealOps<R>::u01(kOO, sw.at(pos++)));
+            break;
+    }
+    return O::mul(k.beta, r);
+}
+
+template <typename R>
+struct GammaTraits {
+    static constexpr int K = 8192 / static_cast<int>(sizeof(R));
+};
+
+// Shared memory of the chunk loop (after the generator's own table): the
+// staged words of one chunk, reused for the redraw list of algorithm N.
+template <class G, typename W, typename R>
+struct GammaSmem {
+    static constexpr int K = GammaTraits<R>::K;
+    static constexpr int WPB = G::kWords / WordView<W>::kPer32;
+    static constexpr int kStageBlocks = (2 * K + 2) / WPB + 2;
+    static constexpr int kStageBytes = kStageBlocks * G::kWords * 4;
+    static constexpr int kListBytes = K * (4 + 2 * static_cast<int>(sizeof(R)));
+    static constexpr int kBytes = kStageBytes > kListBytes ? kStageBytes : kListBytes;
+};
+
+// One chunk of n <= K values at stream word `pos`; accepted values go to
+// out[0, m).  Returns m; advances `pos` and `eng` past the chunk's words.
+template <class G, typename W, typename R, int THREADS>
+__device__ uint32_t gamma_chunk(const G &g, const GammaParam<R> &k, const Ctr &B, uint32_t off, uint64_t &pos,
+    DevEngine<G::kCtrWords> &eng, uint32_t n, R *out, unsigned char *smem, uint32_t *shr, uint64_t *sh_pos)
+{
+    using O = GOps<R>;
+    using S = GammaSmem<G, W, R>;
+    constexpr int K = S::K, WPB = S::WPB, EPT = K / THREADS;
+    constexpr uint32_t M = static_cast<uint32_t>(WPB);
+    const R d = k.d, c = k.c, beta = k.beta;
+    // ---- stage this chunk's words
+    const uint64_t nw = (k.alg <= 1) ? 2ull * n : (k.alg == 2 ? 2ull * n + ((n & 1u) ? 2 : 0) : n);
+    uint32_t *st32 = reinterpret_cast<uint32_t *>(smem);
+    const W *st = reinterpret_cast<const W *>(st32);
+    const uint64_t a0 = static_cast<uint64_t>(off) + pos, b0 = a0 / WPB;
+    const uint32_t s0 = static_cast<uint32_t>(a0 % WPB);
+    const int nb = static_cast<int>((s0 + nw + WPB - 1) / WPB);
+    for (int i = threadIdx.x; i < nb; i += THREADS) {
+        uint32_t blk[G::kWords];
+        g.block(ctr_add(B, b0 + i, G::kCtrWords), blk);
+#pragma unroll
+        for (int q = 0; q < G::kWords; ++q) st32[i * G::kWords + q] = blk[q];
+    }
+    __syncthreads();
+    R x[EPT];
+    bool acc[EPT];
+    uint32_t got = 0;
+    if (k.alg == 3) {
+#pragma unroll
+        for (int j = 0; j < EPT; ++j) {
+            const uint32_t i = threadIdx.x + j * THREADS;
+            if (i < n) out[i] = O::mul(-beta, O::log(RealOps<R>::u01(kOO, st[s0 + i])));
+        }
+        got = n;
+        __syncthreads();
+    } else if (k.alg <= 1) {
+#pragma unroll
+        for (int j = 0; j < EPT; ++j) {
+            const uint32_t i = threadIdx.x + j * THREADS;
+            acc[j] = false;
+            if (i >= n) continue;
+            R u = RealOps<R>::u01(kOO, st[s0 + i]);
+            R e = RealOps<R>::u01(kOO, st[s0 + n + i]);
+            if (k.alg == 0) {
+                e = O::mul(static_cast<R>(-1), O::log(e));
+                if (u > d) {
+                    const R t = O::mul(c, O::sub(static_cast<R>(1), u));
+                    u = -O::log(t);
+                    e = O::add(e, u);
+                    u = O::add(d, O::mul(k.alpha, u));
+                }
+                R xv = O::exp(O::mul(c, O::log(u)));
+                const R ua = fabs(xv);
+                x[j] = O::mul(beta, xv);
+                acc[j] = ua < e;
+            } else {
+                u = O::mul(static_cast<R>(-1), O::log(u));
+                e = O::mul(static_cast<R>(-1), O::log(e));
+                const R xv = O::exp(O::mul(c, O::log(u)));
+                u = O::add(u, e);
+                e = O::add(d, xv);
+                x[j] = O::mul(beta, xv);
+                acc[j] = u > e;
+            }
+        }
+        __syncthreads();
+    } else {
+        // ---- algorithm N: u, the batch normals w, v = fma(c, w, 1)
+        R u[EPT], w[EPT], v[EPT];
+        const uint32_t nu = n / 2;
+        const uint64_t q0 = s0 + n;  // first normal word in the staging buffer
+#pragma unroll
+        for (int j = 0; j < EPT; ++j) {
+            const uint32_t i = threadIdx.x + j * THREADS;
+            u[j] = w[j] = v[j] = 0;
+            if (i >= n) continue;
+            u[j] = RealOps<R>::u01(kOO, st[s0 + i]);
+            R z;
+            if (i < 2 * nu) {
+                const uint32_t p = i < nu ? i : i - nu;
+                const R u1 = RealOps<R>::u01(kOC, st[q0 + p]);
+                const R u2 = O::mul(O::kTwoPi, RealOps<R>::u01(kOC, st[q0 + nu + p]));
+                const R s = O::sqrt(O::mul(static_cast<R>(-2), O::log(u1)));
+                R sn, cs;
+                O::sincos(u2, &sn, &cs);
+                z = O::mul(s, i < nu ? sn : cs);
+            } else {
+                // odd n: the last normal from the two words after the batch
+                const R a = RealOps<R>::u01(kOC, st[q0 + n]);
+                const R b = RealOps<R>::u01(kOC, st[q0 + n + 1]);
+                const R s = O::mul(static_cast<R>(1), O::sqrt(O::mul(static_cast<R>(-2), O::log(a))));
+                R sn, cs;
+                O::sincos(O::mul(O::kTwoPi, b), &sn, &cs);
+                z = O::add(static_cast<R>(0), O::mul(s, cs));
+            }
+            w[j] = z;
+            v[j] = O::fma(c, z, static_cast<R>(1));
+        }
+        // ---- redraws of v <= 0, in index order, by one thread
+        uint32_t *lidx = reinterpret_cast<uint32_t *>(smem);
+        R *lw = reinterpret_cast<R *>(smem + K * 4);
+        R *lv = lw + K;
+        int rk[EPT];
+        uint32_t nred = 0;
+#pragma unroll
+        for (int j = 0; j < EPT; ++j) {
+            const uint32_t i = threadIdx.x + j * THREADS;
+            const bool f = i < n && v[j] <= 0;
+            uint32_t tot;
+            const uint32_t r = block_rank<THREADS>(f, shr, &tot);  // syncs: staging reads are done
+            rk[j] = f ? static_cast<int>(nred + r) : -1;
+            if (f) lidx[nred + r] = i;
+            nred += tot;
+        }
+        if (nred) {
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                ScalarWords<G, W> sw{&g, B, off};
+                uint64_t sp = pos + nw;
+                ScalarNormal<R> rn;
+                for (uint32_t q = 0; q < nred; ++q) {
+                    R wz, vz;
+                    do {
+                        wz = rn(sw, sp);
+                        vz = O::add(static_cast<R>(1), O::mul(c, wz));
+                    } while (vz <= 0);
+                    lw[q] = wz;
+                    lv[q] = vz;
+                }
+                *sh_pos = sp - (pos + nw);
+            }
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < EPT; ++j) {
+                if (rk[j] >= 0) {
+                    w[j] = lw[rk[j]];
+                    v[j] = lv[rk[j]];
+                }
+            }
+        }
+        const uint64_t nscalar = nred ? *sh_pos : 0;
+        const R db = O::mul(d, beta);
+#pragma unroll
+        for (int j = 0; j < EPT; ++j) {
+            const uint32_t i = threadIdx.x + j * THREADS;
+            acc[j] = false;
+            if (i >= n) continue;
+            R e = O::mul(v[j], v[j]);
+            const R vv = O::mul(v[j], e);
+            e = O::mul(w[j], w[j]);
+            e = O::mul(e, e);
+            e = O::fma(-O::k0331, e, static_cast<R>(1));
+            x[j] = O::mul(db, vv);
+            if (u[j] < e) {
+                acc[j] = true;
+            } else {
+                const R a = O::div(O::mul(w[j], w[j]), static_cast<R>(2));
+                const R b = O::add(O::sub(static_cast<R>(1), vv), O::log(vv));
+                e = O::add(a, O::mul(d, b));
+                acc[j] = O::log(u[j]) < e;
+            }
+        }
+        __syncthreads();  // every thread has read nscalar
+        // engine calls of the N chunk: uniforms, normals (+2 odd words), redraw words
+        eng.batch(n, K, M);
+        if (n == static_cast<uint32_t>(K)) {
+            eng.call(K, M);
+            eng.call(0, M);
+            eng.call(0, M);
+        } else {
+            eng.call(n, M);
+        }
+        if (n & 1u) {
+            eng.call(1, M);
+            eng.call(1, M);
+        }
+        for (uint64_t q = 0; q < nscalar; ++q) eng.call(1, M);
+        pos += nw + nscalar;
+    }
+    if (k.alg != 2) {
+        eng.batch(k.alg <= 1 ? 2ull * n : n, K, M);
+        pos += nw;
+    }
+    if (k.alg == 3) return got;
+    // ---- compaction of the accepted values, in index order
+    uint32_t m = 0;
+#pragma unroll
+    for (int j = 0; j < EPT; ++j) {
+        uint32_t tot;
+        const uint32_t r = block_rank<THREADS>(acc[j], shr, &tot);
+        if (acc[j]) out[m + r] = x[j];
+        m += tot;
+    }
+    return m;
+}
+
+// gamma_distribution (:277-302) for `nstreams` streams of n values.  Stream s
+// writes r + s * n; its engine starts at (ctr0 with word 1 = s, empty buffer)
+// when `blocks` is set, else at the engine state given (one stream), whose
+// final state goes to *state_out.
+template <class G, typename W, typename R, int THREADS>
+__global__ void __launch_bounds__(THREADS) k_gamma(G g, Ctr ctr0, uint32_t idx0, int blocks, uint64_t nstreams,
+    uint64_t n, const GammaParam<R> *params, R *r, Ctr *ctr_out, uint32_t *idx_out)
+{
+    using S = GammaSmem<G, W, R>;
+    constexpr int K = S::K;
+    constexpr uint32_t M = static_cast<uint32_t>(S::WPB);
+    __shared__ uint32_t shr[THREADS / 32 + 1];
+    __shared__ uint64_t sh_pos;
+    extern __shared__ __align__(16) unsigned char gamma_dyn[];
+    g.prepare();
+    unsigned char *smem = gamma_dyn + G::kDynSmem;
+    for (uint64_t sidx = blockIdx.x; sidx < nstreams; sidx += gridDim.x) {
+        const GammaParam<R> k = params[blocks ? sidx : 0];
+        DevEngine<G::kCtrWords> eng;
+        eng.ctr = ctr0;
+        eng.idx = idx0;
+        if (blocks) {
+            eng.ctr.w[0] = 0;
+            eng.ctr.w[1] = sidx;
+            eng.ctr.w[2] = eng.ctr.w[3] = 0;
+            eng.idx = M;
+        }
+        // first word of the stream
+        Ctr B = eng.ctr;
+        uint32_t off = eng.idx;
+        if (eng.idx >= M) {
+            B = ctr_add(eng.ctr, 1, G::kCtrWords);
+            off = 0;
+        }
+        uint64_t pos = 0, left = n;
+        R *o = r + sidx * n;
+        while (left > static_cast<uint64_t>(K)) {
+            const uint32_t m = gamma_chunk<G, W, R, THREADS>(g, k, B, off, pos, eng, K, o, smem, shr, &sh_pos);
+            if (m == 0) break;
+            left -= m;
+            o += m;
+        }
+        const uint32_t m = gamma_chunk<G, W, R, THREADS>(g, k, B, off, pos, eng, static_cast<uint32_t>(left), o,
+            smem, shr, &sh_pos);
+        left -= m;
+        o += m;
+        if (left && threadIdx.x == 0) {
+            ScalarWords<G, W> sw{&g, B, off};
+            uint64_t sp = pos;
+            for (uint64_t i = 0; i < left; ++i) o[i] = gamma_scalar<R>(k, sw, sp);
+            for (uint64_t q = pos; q < sp; ++q) eng.call(1, M);
+        }
+        if (!blocks && threadIdx.x == 0) {
+            *ctr_out = eng.ctr;
+            *idx_out = eng.idx;
+        }
+        __syncthreads();
+    }
+}
+
+constexpr int kGammaThreads = 256;
+
+template <typename R>
+int gamma_impl(mckl_b200_engine_t *e, bool blocks, size_t nstreams, size_t n, const GammaParam<R> *hparams,
+    size_t nparams, R *r, void *stream)
+{
+    cudaStream_t s = as_stream(stream);
+    // device copies: per-stream constants, final engine state
+    const size_t pbytes = align256(nparams * sizeof(GammaParam<R>));
+    char *scr = static_cast<char *>(scratch(6, pbytes + 256, s));
+    if (!scr) return MCKL_B200_ERR_NOMEM;
+    auto *dparams = reinterpret_cast<GammaParam<R> *>(scr);
+    Ctr *dctr = reinterpret_cast<Ctr *>(scr + pbytes);
+    uint32_t *didx = reinterpret_cast<uint32_t *>(scr + pbytes + sizeof(Ctr));
+    MB_CUDA(cudaMemcpyAsync(dparams, hparams, nparams * sizeof(GammaParam<R>), cudaMemcpyHostToDevice, s));
+    const Ctr c0 = ctr_of(*e);
+    const uint32_t idx0 = e->index;
+    const bool w64 = geom(e->kind).rbytes == 8;
+    int rc = with_generator(*e, [&](auto g) {
+        using G = decltype(g);
+        auto run = [&](auto wtag) {
+            using W = decltype(wtag);
+            using S = GammaSmem<G, W, R>;
+            auto kern = k_gamma<G, W, R, kGammaThreads>;
+            const int dyn = G::kDynSmem + S::kBytes;
+            MB_CUDA(allow_dyn_smem(kern, dyn));
+            int per_sm = 0;
+            MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kGammaThreads, dyn));
+            int dev = 0, sms = 148;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            const uint64_t cap = static_cast<uint64_t>(std::max(1, per_sm)) * sms;
+            const unsigned grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(nstreams, cap)));
+            kern<<<grid, kGammaThreads, dyn, s>>>(g, c0, idx0, blocks ? 1 : 0, nstreams, n, dparams, r, dctr, didx);
+            MB_LAUNCH_CHECK();
+            return MCKL_B200_OK;
+        };
+        if (w64) return run(uint64_t{});
+        return run(uint32_t{});
+    });
+    if (rc != MCKL_B200_OK) return rc;
+    if (!blocks) {
+        Ctr hc;
+        uint32_t hi = 0;
+        MB_CUDA(cudaMemcpyAsync(&hc, dctr, sizeof(Ctr), cudaMemcpyDeviceToHost, s));
+        MB_CUDA(cudaMemcpyAsync(&hi, didx, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        MB_CUDA(cudaStreamSynchronize(s));
+        set_ctr(*e, hc);
+        e->index = hi;
+    }
+    return MCKL_B200_OK;
+}
+
+template <typename R>
+int gamma_one(mckl_b200_engine_t *e, size_t n, R *r, R alpha, R beta, void *stream)
+{
+    MB_CHECK_ARG(e != nullptr, "null engine");
+    MB_CHECK_ARG(kind_valid(e->kind), "invalid engine kind");
+    MB_CHECK_ARG(n == 0 || r != nullptr, "null output");
+    MB_CHECK_ARG(alpha > 0 && beta > 0, "alpha and beta must be positive");
+    if (n == 0) return MCKL_B200_OK;
+    const GammaParam<R> p = gamma_param<R>(alpha, beta);
+    return gamma_impl<R>(e, false, 1, n, &p, 1, r, stream);
+}
+
+template <typename R>
+int gamma_blocks(const mckl_b200_engine_t *e, size_t nblocks, size_t block, const double *alpha, double beta,
+    R *r, void *stream)
+{
+    MB_CHECK_ARG(e != nullptr && alpha != nullptr, "null argument");
+    MB_CHECK_ARG(kind_valid(e->kind), "invalid engine kind");
+    MB_CHECK_ARG(nblocks == 0 || block == 0 || r != nullptr, "null output");
+    MB_CHECK_ARG(beta > 0, "beta must be positive");
+    if (nblocks == 0 || block == 0) return MCKL_B200_OK;
+    std::vector<GammaParam<R>> p(nblocks);
+    for (size_t b = 0; b < nblocks; ++b) {
+        MB_CHECK_ARG(alpha[b] > 0, "alpha must be positive");
+        p[b] = gamma_param<R>(static_cast<R>(alpha[b]), static_cast<R>(beta));
+    }
+    mckl_b200_engine_t copy = *e;
+    return gamma_impl<R>(&copy, true, nblocks, block, p.data(), nblocks, r, stream);
+}
+
+}  // namespace
+
+}  // namespace mckl_b200
+
+using namespace mckl_b200;
+
+extern "C" {
+
+int mckl_b200_gamma_f32(mckl_b200_engine_t *e, size_t n, float *r, float alpha, float beta, void *stream)
+{
+    return gamma_one<float>(e, n, r, alpha, beta, stream);
+}
+
+int mckl_b200_gamma_f64(mckl_b200_engine_t *e, size_t n, double *r, double alpha, double beta, void *stream)
+{
+    return gamma_one<double>(e, n, r, alpha, beta, stream);
+}
+
+int mckl_b200_gamma_blocks_f32(const mckl_b200_engine_t *e, size_t nblocks, size_t block, const double *alpha,
+    double beta, float *r, void *stream)
+{
+    return gamma_blocks<float>(e, nblocks, block, alpha, beta, r, stream);
+}
+
+int mckl_b200_gamma_blocks_f64(const mckl_b200_engine_t *e, size_t nblocks, size_t block, const double *alpha,
+    double beta, double *r, void *stream)
+{
+    return gamma_blocks<double>(e, nblocks, block, alpha, beta, r, stream);
+}
+
+}  // extern "C"

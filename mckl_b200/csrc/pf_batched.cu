@@ -90,22 +90,134 @@ __device__ __forceinline__ T block_max(T v, T *sh)
     return r;
 }
 
+// Online log-sum-exp accumulator of one thread: s = sum exp(v - m),
+// q = sum exp(2 (v - m)) over the values seen, m their running maximum.  The
+// terms are evaluated in the propagation type, summed in FP64; a new maximum
+// rescales the sums by an FP64 exp (values arrive in groups of up to eight,
+// so this happens a few times per thread and step).
+template <typename R>
+struct Lse {
+    R m = -INFINITY;
+    double s = 0.0, q = 0.0;
+
+    template <int K>
+    __device__ __forceinline__ void add(const R (&v)[K], int lo, int hi)
+    {
+        R gm = -INFINITY;
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            if (k >= lo && k < hi) gm = fmax(gm, v[k]);
+        if (gm > m) {
+            const double sc = (m == -INFINITY) ? 0.0 : ::exp(static_cast<double>(m) - static_cast<double>(gm));
+            s *= sc;
+            q *= sc * sc;
+            m = gm;
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (k >= lo && k < hi) {
+                const double e = static_cast<double>(Math<R>::exp(v[k] - m));
+                s += e;
+                q += e * e;
+            }
+        }
+    }
+};
+
+// The combined (max, sum, sum of squares) of a CTA's accumulators.
+template <typename R>
+__device__ __forceinline__ void block_lse(const Lse<R> &a, R *shr, double *shd, R *M, double *S, double *Q)
+{
+    const R mm = block_max(a.m, shr);
+    const double sc = (a.m == -INFINITY) ? 0.0 : ::exp(static_cast<double>(a.m) - static_cast<double>(mm));
+    *M = mm;
+    *S = block_sum(a.s * sc, shd);
+    if (Q) *Q = block_sum(a.q * sc * sc, shd);
+}
+
+// One Box-Muller pair of one filter at step t: the noise from a radius and an
+// angle word, the AR(1) move of particles p0 and p1, their new log-weights
+// (old log-weight minus the previous step's maximum, plus the observation's
+// log-density; zero old weights after a resampling) and, for the shadow, the
+// same in FP64.  Returns the two log-weights in v[0], v[1].
+template <typename R, bool SHADOW>
+struct Step {
+    R *x, *l;
+    double *xs, *ls;
+    R phi, sx, sd0, lconst, hinv, yt, lshift;
+    double phi_d, sx_d, sd0_d, lconst_d, hinv_d, yt_d, lshift_s;
+    bool init, flat;
+
+    __device__ __forceinline__ void pair(uint32_t wrad, uint32_t wang, uint64_t p0, uint64_t p1, R *v, double *vs) const
+    {
+        const R rr = Math<R>::radius(u01oc<R>(wrad));
+        R sn, cs;
+        Math<R>::sincos2pi(u01oc<R>(wang), &sn, &cs);
+        one(rr * sn, p0, v[0]);
+        one(rr * cs, p1, v[1]);
+        if constexpr (SHADOW) {
+            const double rd = Math<double>::radius(u01oc<double>(wrad));
+            double snd, csd;
+            Math<double>::sincos2pi(u01oc<double>(wang), &snd, &csd);
+            one_shadow(rd * snd, p0, vs[0]);
+            one_shadow(rd * csd, p1, vs[1]);
+        }
+    }
+
+    __device__ __forceinline__ void one(R e, uint64_t p, R &v) const
+    {
+        if (init) {
+            x[p] = sd0 * e;
+            return;
+        }
+        const R xn = phi * x[p] + sx * e;
+        x[p] = xn;
+        const R r = yt - xn;
+        const R lo = flat ? R(0) : l[p] - lshift;
+        v = lo + (lconst - r * r * hinv);
+        l[p] = v;
+    }
+
+    __device__ __forceinline__ void one_shadow(double e, uint64_t p, double &v) const
+    {
+        if (init) {
+            xs[p] = sd0_d * e;
+            return;
+        }
+        const double xn = phi_d * xs[p] + sx_d * e;
+        xs[p] = xn;
+        const double r = yt_d - xn;
+        const double lo = flat ? 0.0 : ls[p] - lshift_s;
+        v = lo + (lconst_d - r * r * hinv_d);
+        ls[p] = v;
+    }
+};
+
 // SHADOW (with R = float): every particle also carries an FP64 copy that is
 // propagated with the same uniforms, weighted in FP64 and resampled with the
 // FP32 run's decisions and parent indices; its log-likelihood isolates the
 // FP32 arithmetic error from the Monte Carlo divergence a flipped ancestor
 // would otherwise start.
+//
+// Work split of one step: the Normal(0,1) draws of a filter are 1024-value
+// chunks (radius word i, angle word 512 + i of the chunk, as
+// normal_distribution lays them out).  A full chunk is covered by 129 units;
+// unit g owns the radius words of Philox block (chunk start / 4) + g and the
+// angle words of the block 128 further on, i.e. up to four pairs for two
+// Philox blocks (a quarter block per particle).  The last partial chunk and an
+// odd last particle are drawn word by word.
 template <typename R, int THREADS, bool SHADOW>
 __global__ void __launch_bounds__(THREADS) k_pf_batched(const BatchedFilter *filt, const int *order, int nf,
-    const double *y, int T, double threshold, R *xa, R *xb, R *lw, uint32_t *cnt, uint32_t *scanS,
-    uint32_t *epos, double *loglik, uint32_t *nresampled, int *queue, double *xsa, double *xsb, double *lws,
+    const double *y, int T, double threshold, R *xa, R *xb, R *lw, uint32_t *scanS, uint32_t *epos,
+    double *loglik, uint32_t *nresampled, int *queue, double *xsa, double *xsb, double *lws,
     double *loglik_shadow)
 {
     __shared__ double shd[33];
     __shared__ R shr[33];
     __shared__ unsigned long long shu[33];
+    __shared__ uint32_t shj[THREADS + 1];
     __shared__ int sh_f;
-    // work arrays are indexed by each filter's particle offset
+    constexpr uint64_t kUnits = 129;  // units per full chunk
     while (true) {
         if (threadIdx.x == 0) {
             const int k = atomicAdd(queue, 1);
@@ -117,150 +229,114 @@ __global__ void __launch_bounds__(THREADS) k_pf_batched(const BatchedFilter *fil
         if (f < 0) break;
         const BatchedFilter F = filt[f];
         const uint64_t N = F.n;
-        R *x = xa + F.off, *x2 = xb + F.off, *l = lw + F.off;
-        double *xs = SHADOW ? xsa + F.off : nullptr, *xs2 = SHADOW ? xsb + F.off : nullptr;
-        double *ls = SHADOW ? lws + F.off : nullptr;
-        const double phi_d = F.phi, sx_d = F.sx, sd0_d = F.sd0, lconst_d = F.lconst, hinv_d = F.hinv;
-        double Ls_prev = log(static_cast<double>(N)), lls_sum = 0.0;
-        uint32_t *ct = cnt + F.off, *sS = scanS + F.off, *ep = epos + F.off;
+        R *xc = xa + F.off, *xn = xb + F.off;
+        double *xsc = SHADOW ? xsa + F.off : nullptr, *xsn = SHADOW ? xsb + F.off : nullptr;
+        uint32_t *sS = scanS + F.off, *ep = epos + F.off;
         const PhiloxGen gm{F.mkey[0], F.mkey[1]}, gr{F.rkey[0], F.rkey[1]};
         const uint64_t per_step = N + (N & 1) * 2;  // words of one normal_distribution(N) call
-        const uint64_t m = N / 1024, tail = N % 1024;
-        const R phi = static_cast<R>(F.phi), sx = static_cast<R>(F.sx), sd0 = static_cast<R>(F.sd0);
-        const R lconst = static_cast<R>(F.lconst), hinv = static_cast<R>(F.hinv);
+        const uint64_t m = N / 1024, tail = N % 1024, nu_tail = tail / 2;
+        const uint64_t units = m * kUnits + nu_tail;
+        Step<R, SHADOW> st;
+        st.l = lw + F.off;
+        st.ls = SHADOW ? lws + F.off : nullptr;
+        st.phi = static_cast<R>(F.phi);
+        st.sx = static_cast<R>(F.sx);
+        st.sd0 = static_cast<R>(F.sd0);
+        st.lconst = static_cast<R>(F.lconst);
+        st.hinv = static_cast<R>(F.hinv);
+        st.phi_d = F.phi;
+        st.sx_d = F.sx;
+        st.sd0_d = F.sd0;
+        st.lconst_d = F.lconst;
+        st.hinv_d = F.hinv;
+        st.lshift = 0;
+        st.lshift_s = 0.0;
+        st.flat = true;
         double L_prev = log(static_cast<double>(N)), ll_sum = 0.0;
+        double Ls_prev = L_prev, lls_sum = 0.0;
         uint64_t events = 0;
         for (int t = 0; t <= T; ++t) {
             const uint64_t P = static_cast<uint64_t>(t) * per_step;
-            const R yt = static_cast<R>(y[static_cast<uint64_t>(f) * (T + 1) + t]);
-            // ---- noise, propagation, log-likelihood, log-weights; running max
-            R vmax = -INFINITY;
-            double vmax_s = -INFINITY;
-            const double yt_d = y[static_cast<uint64_t>(f) * (T + 1) + t];
-            const uint64_t pairs = m * 512 + tail / 2;
-            for (uint64_t q = threadIdx.x; q < pairs; q += THREADS) {
-                const uint64_t c = q / 512, i = q % 512;
-                const uint64_t nu = (c < m ? 1024 : tail) / 2;
-                const uint64_t base = P + c * 1024;
-                WordCache wc{~0ull, {0, 0, 0, 0}};
-                const uint32_t wrad = word_at(gm, base + i, wc);
-                const uint32_t wang = word_at(gm, base + nu + i, wc);
-                const R s = Math<R>::radius(u01oc<R>(wrad));
-                R sn, cs;
-                Math<R>::sincos2pi(u01oc<R>(wang), &sn, &cs);
-                const uint64_t p0 = c * 1024 + i, p1 = c * 1024 + nu + i;
-                if constexpr (SHADOW) {
-                    const double sd = Math<double>::radius(u01oc<double>(wrad));
-                    double snd, csd;
-                    Math<double>::sincos2pi(u01oc<double>(wang), &snd, &csd);
-                    const double e0 = sd * snd, e1 = sd * csd;
-                    double x0, x1;
-                    if (t == 0) {
-                        x0 = sd0_d * e0;
-                        x1 = sd0_d * e1;
-                        ls[p0] = 0;
-                        ls[p1] = 0;
-                    } else {
-                        x0 = phi_d * xs[p0] + sx_d * e0;
-                        x1 = phi_d * xs[p1] + sx_d * e1;
-                        const double r0 = yt_d - x0, r1 = yt_d - x1;
-                        const double l0 = ls[p0] + (lconst_d - r0 * r0 * hinv_d);
-                        const double l1 = ls[p1] + (lconst_d - r1 * r1 * hinv_d);
-                        ls[p0] = l0;
-                        ls[p1] = l1;
-                        vmax_s = fmax(vmax_s, fmax(l0, l1));
+            st.x = xc;
+            st.xs = xsc;
+            st.init = (t == 0);
+            st.yt_d = y[static_cast<uint64_t>(f) * (T + 1) + t];
+            st.yt = static_cast<R>(st.yt_d);
+            Lse<R> acc;
+            Lse<double> accs;
+            // ---- noise, propagation, log-weights, online normaliser
+            for (uint64_t u = threadIdx.x; u < units; u += THREADS) {
+                R v[8];
+                double vs[8];
+                if (u < m * kUnits) {
+                    const uint64_t c = u / kUnits, g = u % kUnits;
+                    const uint64_t base = P + c * 1024;
+                    const uint64_t B = (base >> 2) + g;
+                    const int i0 = static_cast<int>(4 * g) - static_cast<int>(base & 3);
+                    uint32_t wr[4], wa[4];
+                    gm.block(Ctr{{B + 1, 0, 0, 0}}, wr);
+                    gm.block(Ctr{{B + 129, 0, 0, 0}}, wa);
+                    const int lo = i0 < 0 ? -i0 : 0, hi = i0 + 4 > 512 ? 512 - i0 : 4;
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        if (j >= lo && j < hi) {
+                            const uint64_t p0 = c * 1024 + static_cast<uint64_t>(i0 + j);
+                            st.pair(wr[j], wa[j], p0, p0 + 512, v + 2 * j, vs + 2 * j);
+                        }
                     }
-                    xs[p0] = x0;
-                    xs[p1] = x1;
-                }
-                const R e0 = s * sn, e1 = s * cs;
-                R x0, x1;
-                if (t == 0) {
-                    x0 = sd0 * e0;
-                    x1 = sd0 * e1;
-                    l[p0] = 0;
-                    l[p1] = 0;
+                    if (t > 0) {
+                        acc.add(v, 2 * lo, 2 * hi);
+                        if constexpr (SHADOW) accs.add(vs, 2 * lo, 2 * hi);
+                    }
                 } else {
-                    x0 = phi * x[p0] + sx * e0;
-                    x1 = phi * x[p1] + sx * e1;
-                }
-                x[p0] = x0;
-                x[p1] = x1;
-                if (t > 0) {
-                    const R r0 = yt - x0, r1 = yt - x1;
-                    const R l0 = l[p0] + (lconst - r0 * r0 * hinv);
-                    const R l1 = l[p1] + (lconst - r1 * r1 * hinv);
-                    l[p0] = l0;
-                    l[p1] = l1;
-                    vmax = fmax(vmax, fmax(l0, l1));
+                    const uint64_t i = u - m * kUnits, base = P + m * 1024;
+                    WordCache wc{~0ull, {0, 0, 0, 0}};
+                    const uint32_t wrad = word_at(gm, base + i, wc);
+                    const uint32_t wang = word_at(gm, base + nu_tail + i, wc);
+                    st.pair(wrad, wang, m * 1024 + i, m * 1024 + nu_tail + i, v, vs);
+                    if (t > 0) {
+                        acc.add(v, 0, 2);
+                        if constexpr (SHADOW) accs.add(vs, 0, 2);
+                    }
                 }
             }
             if ((N & 1) && threadIdx.x == THREADS - 1) {
                 // odd N: the last particle from the two words after the chunks
                 WordCache wc{~0ull, {0, 0, 0, 0}};
-                const R u = u01oc<R>(word_at(gm, P + N, wc));
-                const R v = u01oc<R>(word_at(gm, P + N + 1, wc));
-                const R e = Math<R>::radius(u) * Math<R>::cos2pi(v);
-                const uint64_t p = N - 1;
-                if constexpr (SHADOW) {
-                    WordCache wd{~0ull, {0, 0, 0, 0}};
-                    const double ud = u01oc<double>(word_at(gm, P + N, wd));
-                    const double vd = u01oc<double>(word_at(gm, P + N + 1, wd));
-                    const double ed = Math<double>::radius(ud) * Math<double>::cos2pi(vd);
-                    const double xn = t == 0 ? sd0_d * ed : phi_d * xs[p] + sx_d * ed;
-                    xs[p] = xn;
-                    if (t == 0) {
-                        ls[p] = 0;
-                    } else {
-                        const double r = yt_d - xn;
-                        const double ln = ls[p] + (lconst_d - r * r * hinv_d);
-                        ls[p] = ln;
-                        vmax_s = fmax(vmax_s, ln);
-                    }
-                }
-                const R xn = t == 0 ? sd0 * e : phi * x[p] + sx * e;
-                x[p] = xn;
-                if (t == 0) l[p] = 0;
+                const uint32_t w0 = word_at(gm, P + N, wc), w1 = word_at(gm, P + N + 1, wc);
+                R v[1];
+                double vs[1];
+                st.one(Math<R>::radius(u01oc<R>(w0)) * Math<R>::cos2pi(u01oc<R>(w1)), N - 1, v[0]);
+                if constexpr (SHADOW)
+                    st.one_shadow(Math<double>::radius(u01oc<double>(w0)) * Math<double>::cos2pi(u01oc<double>(w1)),
+                        N - 1, vs[0]);
                 if (t > 0) {
-                    const R r = yt - xn;
-                    const R ln = l[p] + (lconst - r * r * hinv);
-                    l[p] = ln;
-                    vmax = fmax(vmax, ln);
+                    acc.add(v, 0, 1);
+                    if constexpr (SHADOW) accs.add(vs, 0, 1);
                 }
             }
             if (t == 0) {
                 __syncthreads();
                 continue;
             }
-            const R lmax = block_max(vmax, shr);
-            // ---- FP64 normaliser: S = sum exp(l - lmax), Q = sum exp^2; the
-            // log-weights are shifted by lmax (kept <= 0) and the FP64 log
-            // normaliser of the shifted weights carried to the next step
-            double S = 0.0, Q = 0.0;
-            for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
-                const R lp = l[p] - lmax;
-                l[p] = lp;
-                const double e = static_cast<double>(Math<R>::exp(lp));
-                S += e;
-                Q += e * e;
-            }
-            S = block_sum(S, shd);
-            Q = block_sum(Q, shd);
-            const double L = static_cast<double>(lmax) + log(S);
+            // ---- FP64 normaliser: S = sum exp(l - M), Q = sum exp^2; the
+            // log normaliser of the weights relative to M is carried to the
+            // next step, whose log-weights start from l - M
+            R M;
+            double S, Q;
+            block_lse(acc, shr, shd, &M, &S, &Q);
+            const double L = static_cast<double>(M) + log(S);
             ll_sum += L - L_prev;
             L_prev = log(S);
             if constexpr (SHADOW) {
-                const double lmax_s = block_max(vmax_s, shd);
-                double Ss = 0.0;
-                for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
-                    const double lp = ls[p] - lmax_s;
-                    ls[p] = lp;
-                    Ss += exp(lp);
-                }
-                Ss = block_sum(Ss, shd);
-                lls_sum += lmax_s + log(Ss) - Ls_prev;
+                double Ms, Ss;
+                block_lse<double>(accs, shd, shd, &Ms, &Ss, nullptr);
+                lls_sum += Ms + log(Ss) - Ls_prev;
                 Ls_prev = log(Ss);
+                st.lshift_s = Ms;
             }
+            st.lshift = M;
+            st.flat = false;
             const double ess = S * S / Q;
             if (!(ess < static_cast<double>(N) * threshold)) continue;
             // ---- systematic resampling
@@ -277,41 +353,46 @@ __global__ void __launch_bounds__(THREADS) k_pf_batched(const BatchedFilter *fil
             const double delta = 1.0 / static_cast<double>(N);
             const double ud = U * delta;
             const double invS = 1.0 / S;
-            // inclusive FP64 scan of normalised weights over tiles of THREADS;
-            // count_i = #{j : u_j < c_i}
+            // per tile of THREADS particles: inclusive FP64 scan of the
+            // normalised weights, cumulative counts j_p = #{k : u_k < c_p}
+            // (the lower bound of c_p on the grid fma(k, delta, ud)), the
+            // replication counts j_p - j_{p-1}, and the exclusive scan of
+            // (empty slot, surplus copies) that places the parents
             double carry = 0.0;
+            unsigned long long carry2 = 0;
+            uint32_t jprev = 0;
             for (uint64_t b = 0; b < N; b += THREADS) {
                 const uint64_t p = b + threadIdx.x;
-                const double w = p < N ? static_cast<double>(Math<R>::exp(l[p])) * invS : 0.0;
+                const double w = p < N ? static_cast<double>(Math<R>::exp(st.l[p] - M)) * invS : 0.0;
                 double tot;
                 const double c = carry + block_inclusive_sum(w, shd, &tot);
                 carry += tot;
-                if (p < N) {
-                    // lower bound of c on the grid fma(j, delta, ud), j in [0, N)
+                uint32_t jp = static_cast<uint32_t>(N);
+                if (p + 1 < N) {
                     double jf = ceil((c - ud) * static_cast<double>(N));
                     long long j = jf < 0 ? 0 : (jf > static_cast<double>(N) ? static_cast<long long>(N) : static_cast<long long>(jf));
                     while (j > 0 && fma(static_cast<double>(j - 1), delta, ud) >= c) --j;
                     while (j < static_cast<long long>(N) && fma(static_cast<double>(j), delta, ud) < c) ++j;
-                    ct[p] = static_cast<uint32_t>(p + 1 == N ? N : j);
+                    jp = static_cast<uint32_t>(j);
                 }
-            }
-            __syncthreads();
-            // replication counts -> empty slots and surplus copies (exclusive scans)
-            unsigned long long carry2 = 0;
-            for (uint64_t b = 0; b < N; b += THREADS) {
-                const uint64_t p = b + threadIdx.x;
-                uint32_t rep = 0;
-                if (p < N) rep = ct[p] - (p == 0 ? 0u : ct[p - 1]);
+                shj[threadIdx.x + 1] = jp;
+                if (threadIdx.x == 0) shj[0] = jprev;
+                __syncthreads();
+                const uint32_t rep = p < N ? shj[threadIdx.x + 1] - shj[threadIdx.x] : 0u;
+                jprev = shj[THREADS];
                 const unsigned long long v = p < N ? ((rep == 0 ? 1ull : 0ull) | (static_cast<unsigned long long>(rep > 0 ? rep - 1 : 0) << 32)) : 0ull;
-                unsigned long long tot;
-                const unsigned long long inc = block_inclusive_sum(v, shu, &tot);
+                unsigned long long tot2;
+                const unsigned long long inc = block_inclusive_sum(v, shu, &tot2);
                 const unsigned long long ex = carry2 + inc - v;
-                carry2 += tot;
+                carry2 += tot2;
                 if (p < N) {
                     sS[p] = static_cast<uint32_t>(ex >> 32);
-                    if (rep == 0) ep[ex & 0xffffffffull] = static_cast<uint32_t>(p);
-                    x2[p] = x[p];  // occupied slots keep their particle
-                    if constexpr (SHADOW) xs2[p] = xs[p];
+                    if (rep == 0) {
+                        ep[ex & 0xffffffffull] = static_cast<uint32_t>(p);
+                    } else {
+                        xn[p] = xc[p];  // occupied slots keep their particle
+                        if constexpr (SHADOW) xsn[p] = xsc[p];
+                    }
                 }
             }
             __syncthreads();
@@ -326,21 +407,22 @@ __global__ void __launch_bounds__(THREADS) k_pf_batched(const BatchedFilter *fil
                         hi = mid;
                     }
                 }
-                x2[ep[k]] = x[lo];
-                if constexpr (SHADOW) xs2[ep[k]] = xs[lo];
+                xn[ep[k]] = xc[lo];
+                if constexpr (SHADOW) xsn[ep[k]] = xsc[lo];
             }
             __syncthreads();
-            for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
-                x[p] = x2[p];
-                l[p] = 0;
-                if constexpr (SHADOW) {
-                    xs[p] = xs2[p];
-                    ls[p] = 0;
-                }
+            // the gathered particles become the current ones, with equal weights
+            R *tx = xc;
+            xc = xn;
+            xn = tx;
+            if constexpr (SHADOW) {
+                double *ts = xsc;
+                xsc = xsn;
+                xsn = ts;
             }
+            st.flat = true;
             L_prev = log(static_cast<double>(N));
-            Ls_prev = log(static_cast<double>(N));
-            __syncthreads();
+            Ls_prev = L_prev;
         }
         if (threadIdx.x == 0) {
             loglik[f] = ll_sum;
@@ -355,7 +437,7 @@ template <typename R, int THREADS, bool SHADOW>
 int launch_one(const BatchedArgs &a, const int *order, int nf, int *queue, int ctas, cudaStream_t s)
 {
     k_pf_batched<R, THREADS, SHADOW><<<ctas, THREADS, 0, s>>>(a.filt, order, nf, a.y, a.T, a.threshold,
-        static_cast<R *>(a.xa), static_cast<R *>(a.xb), static_cast<R *>(a.lw), a.cnt, a.scanS, a.epos,
+        static_cast<R *>(a.xa), static_cast<R *>(a.xb), static_cast<R *>(a.lw), a.scanS, a.epos,
         a.loglik, a.nresampled, queue, a.xsa, a.xsb, a.lws, a.loglik_shadow);
     MB_LAUNCH_CHECK();
     return MCKL_B200_OK;
@@ -473,7 +555,7 @@ int mckl_b200_batched_create(mckl_b200_batched_t **out, size_t F, const size_t *
     b->fp64 = (fp64 == 1) ? 1 : 0;
     const size_t rs = b->fp64 ? 8 : 4;
     const size_t bytes = align256(F * sizeof(BatchedFilter)) + align256(F * (T + 1) * 8) + 3 * align256(total * rs) +
-                         3 * align256(total * 4) + align256(F * 8) + align256(F * 4) + align256(F * 4) + 256 +
+                         2 * align256(total * 4) + align256(F * 8) + align256(F * 4) + align256(F * 4) + 256 +
                          (shadow ? 3 * align256(total * 8) + align256(F * 8) : 0);
     if (cudaMalloc(&b->mem, bytes) != cudaSuccess) {
         delete b;
@@ -491,7 +573,6 @@ int mckl_b200_batched_create(mckl_b200_batched_t **out, size_t F, const size_t *
     b->a.xa = take(total * rs);
     b->a.xb = take(total * rs);
     b->a.lw = take(total * rs);
-    b->a.cnt = reinterpret_cast<uint32_t *>(take(total * 4));
     b->a.scanS = reinterpret_cast<uint32_t *>(take(total * 4));
     b->a.epos = reinterpret_cast<uint32_t *>(take(total * 4));
     b->a.loglik = reinterpret_cast<double *>(take(F * 8));

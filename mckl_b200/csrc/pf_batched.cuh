@@ -21,8 +21,8 @@ struct BatchedArgs {
     int T;
     double threshold;
     int fp64;           // 1: propagate in double, 0: in float
-    void *xa, *xb, *lw; // particles, gather buffer, log-weights (float or double)
-    uint32_t *cnt, *scanS, *epos;
+    void *xa, *xb, *lw; // particles (two buffers, swapped at each resampling), log-weights
+    uint32_t *scanS, *epos;
     double *loglik;
     uint32_t *nresampled;
     double *xsa = nullptr, *xsb = nullptr, *lws = nullptr;  // FP64 shadow (FP32 run only)

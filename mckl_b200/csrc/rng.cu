@@ -19,6 +19,7 @@
 #include <unordered_map>
 
 #include "common.cuh"
+#include "dispatch.cuh"
 #include "transforms.cuh"
 
 namespace mckl_b200 {
@@ -88,15 +89,6 @@ static int sm_count()
     return n;
 }
 
-// Allow `kernel` to use `dyn` bytes of dynamic shared memory on top of its
-// static shared memory (needed once the sum passes 48 KiB).
-template <typename K>
-static cudaError_t allow_dyn_smem(K kernel, int dyn)
-{
-    if (dyn == 0) return cudaSuccess;
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
-}
-
 static unsigned grid_for(uint64_t work_items, int threads, int ctas_per_sm)
 {
     const uint64_t need = (work_items + threads - 1) / threads;
@@ -107,26 +99,6 @@ static unsigned grid_for(uint64_t work_items, int threads, int ctas_per_sm)
 // ---------------------------------------------------------------------------
 // device helpers
 // ---------------------------------------------------------------------------
-template <typename W>
-struct WordView;
-
-template <>
-struct WordView<uint32_t> {
-    template <int N>
-    __device__ static uint32_t get(const uint32_t (&b)[N], int j) { return b[j]; }
-    static constexpr int kPer32 = 1;
-};
-
-template <>
-struct WordView<uint64_t> {
-    template <int N>
-    __device__ static uint64_t get(const uint32_t (&b)[N], int j)
-    {
-        return static_cast<uint64_t>(b[2 * j]) | (static_cast<uint64_t>(b[2 * j + 1]) << 32);
-    }
-    static constexpr int kPer32 = 2;
-};
-
 // Write block i into a shared staging buffer with 128-bit stores: consecutive
 // lanes then fill consecutive 16-byte slots (no bank conflicts).
 template <class G>
@@ -349,31 +321,6 @@ __global__ void k_normal_odd(G g, Ctr base, uint64_t a_u, R *dst, R mean, R sd)
 // ---------------------------------------------------------------------------
 // host dispatch
 // ---------------------------------------------------------------------------
-template <class Fn>
-static int with_generator(const mckl_b200_engine_t &e, Fn &&fn)
-{
-    switch (e.kind) {
-        case MCKL_B200_PHILOX4X32:
-        case MCKL_B200_PHILOX4X32_64: {
-            PhiloxGen g{static_cast<uint32_t>(e.key[0]), static_cast<uint32_t>(e.key[1])};
-            return fn(g);
-        }
-        case MCKL_B200_THREEFRY4X64:
-        case MCKL_B200_THREEFRY4X64_64: {
-            ThreefryGen g = ThreefryGen::make(e.key, e.tweak);
-            return fn(g);
-        }
-        case MCKL_B200_ARS:
-        case MCKL_B200_ARS_64: {
-            ArsGen g = ArsGen::make(e.key);
-            return fn(g);
-        }
-        default:
-            set_error("unknown engine kind");
-            return MCKL_B200_ERR_ARG;
-    }
-}
-
 // Launch the word -> output transform F for n outputs from position (B, off).
 template <class G, typename W, class F>
 static int launch_words(const G &g, const Ctr &B, uint32_t off, uint64_t n, typename F::out_t *out,
