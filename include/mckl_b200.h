@@ -229,6 +229,26 @@ int mckl_b200_batched_run_graph(mckl_b200_batched_t *b, void *stream);
 int mckl_b200_batched_results(mckl_b200_batched_t *b, double *loglik, uint32_t *nresampled, void *stream);
 int mckl_b200_batched_shadow(mckl_b200_batched_t *b, double *loglik_fp64, void *stream);
 /* Replace the observations (HOST array of F x (T + 1), copied on `stream`). */
+/* Shadow-run parameters (handles created with fp64 = 2 or 3): the FP64 shadow
+ * follows the main run's resampling decisions and parent indices with its own
+ * (phi, sx, sy) per filter (host arrays of F).  With perturbed parameters it
+ * evaluates the estimate at theta +- h under common random numbers and fixed
+ * ancestors -- the finite differences the adjoint is checked against. */
+int mckl_b200_batched_shadow_params(mckl_b200_batched_t *b, const double *phi, const double *sx, const double *sy);
+
+/* Adjoint: the gradient of each filter's FP64 log-likelihood estimate with
+ * respect to (phi, sx, sy), resampling times and ancestor indices held fixed
+ * (no counterpart in the reference, which has no derivatives).  The forward
+ * pass keeps a checkpoint every `checkpoint_every` steps; the backward pass
+ * replays each block of steps from its checkpoint -- the noise, decisions and
+ * ancestors are recomputed from the counters, not stored -- and sweeps it in
+ * reverse.  Handle created with fp64 = 1.  loglik: F doubles (may be NULL),
+ * grad: F x 3 doubles (d/dphi, d/dsx, d/dsy), both HOST arrays; synchronizes
+ * `stream`.  Device memory: checkpoints 16 B x particles x (T / C + 1) plus
+ * per-SM replay records of C x the largest N x 28 B. */
+int mckl_b200_batched_adjoint(mckl_b200_batched_t *b, int checkpoint_every, double *loglik, double *grad,
+                              void *stream);
+
 /* Autotuner: times the candidate block shapes (threads per CTA x resident CTAs
  * per SM, skipping shapes that do not fit) on this handle's own filters, one
  * full run each, and configures the fastest.  The first `max_trials` trials

@@ -191,6 +191,8 @@ _bt_destroy = _bind("mckl_b200_batched_destroy", [_vp])
 _bt_shadow = _bind("mckl_b200_batched_shadow", [_vp, _vp, _vp])
 _bt_set_y = _bind("mckl_b200_batched_set_y", [_vp, _vp, _vp])
 _bt_autotune = _bind("mckl_b200_batched_autotune", [_vp, _i, _vp, _vp, _vp, _vp, _vp])
+_bt_shadow_params = _bind("mckl_b200_batched_shadow_params", [_vp, _vp, _vp, _vp])
+_bt_adjoint = _bind("mckl_b200_batched_adjoint", [_vp, _i, _vp, _vp, _vp])
 
 
 def _arr(a, dt):
@@ -210,8 +212,9 @@ class BatchedFilters:
                       _arr(mkeys, np.uint32), _arr(rkeys, np.uint32)]
         h = ctypes.c_void_p()
         ptrs = [a.ctypes.data_as(ctypes.c_void_p) for a in self._keep]
+        mode = (3 if fp64 else 2) if shadow else int(bool(fp64))
         _check(_bt_create(ctypes.byref(h), self.F, ptrs[0], self.T, ptrs[1], ptrs[2], ptrs[3], ptrs[4], ptrs[5],
-                          ptrs[6], threshold, 2 if shadow else int(bool(fp64))))
+                          ptrs[6], threshold, mode))
         self.h = h
 
     def config(self, threads=256, ctas_per_sm=4):
@@ -236,6 +239,20 @@ class BatchedFilters:
         n = ctypes.c_int()
         _check(_bt_autotune(self.h, 16, th, cp, ms, ctypes.byref(n), _stream_ptr(stream)))
         return [(th[k], cp[k], ms[k]) for k in range(min(n.value, 16))]
+
+    def set_shadow_params(self, phi, sx, sy):
+        """Parameters of the FP64 shadow (handles made with shadow=True)."""
+        a = [_arr(v, np.float64) for v in (phi, sx, sy)]
+        _check(_bt_shadow_params(self.h, *[v.ctypes.data_as(ctypes.c_void_p) for v in a]))
+
+    def adjoint(self, checkpoint_every=32, stream=None):
+        """(loglik[F], grad[F, 3]): the FP64 estimate and its gradient with
+        respect to (phi, sx, sy), ancestors held fixed (fp64=True handles)."""
+        ll = np.zeros(self.F)
+        g = np.zeros((self.F, 3))
+        _check(_bt_adjoint(self.h, int(checkpoint_every), ll.ctypes.data_as(ctypes.c_void_p),
+                           g.ctypes.data_as(ctypes.c_void_p), _stream_ptr(stream)))
+        return ll, g
 
     def set_y(self, y, stream=None):
         """Copy new observations (host array [F, T + 1]; page-locked for an async copy)."""

@@ -193,21 +193,336 @@ struct Step {
     }
 };
 
-// SHADOW (with R = float): every particle also carries an FP64 copy that is
-// propagated with the same uniforms, weighted in FP64 and resampled with the
-// FP32 run's decisions and parent indices; its log-likelihood isolates the
-// FP32 arithmetic error from the Monte Carlo divergence a flipped ancestor
-// would otherwise start.
-//
-// Work split of one step: the Normal(0,1) draws of a filter are 1024-value
-// chunks (radius word i, angle word 512 + i of the chunk, as
+// Where the Normal(0,1) draws of step t come from.  The draws of a filter
+// are 1024-value chunks (radius word i, angle word 512 + i of the chunk, as
 // normal_distribution lays them out).  A full chunk is covered by 129 units;
 // unit g owns the radius words of Philox block (chunk start / 4) + g and the
 // angle words of the block 128 further on, i.e. up to four pairs for two
-// Philox blocks (a quarter block per particle).  The last partial chunk and an
-// odd last particle are drawn word by word.
+// Philox blocks (a quarter block per particle).  Units past the full chunks
+// are the pairs of the last partial chunk, drawn word by word.
+struct NoiseLayout {
+    static constexpr uint64_t kUnits = 129;  // units per full chunk
+    uint64_t N, m, tail, nu_tail, units, per_step;
+
+    __device__ void init(uint64_t n)
+    {
+        N = n;
+        per_step = N + (N & 1) * 2;  // words of one normal_distribution(N) call
+        m = N / 1024;
+        tail = N % 1024;
+        nu_tail = tail / 2;
+        units = m * kUnits + nu_tail;
+    }
+
+    // Calls pair(wrad, wang, p0, p1, j) for the pairs of unit u at step t
+    // (j: slot of the pair inside the unit) and returns the unit's slot range
+    // [lo, hi).
+    template <class Fn>
+    __device__ __forceinline__ void unit(const PhiloxGen &gm, int t, uint64_t u, int *lo_out, int *hi_out,
+        Fn &&pair) const
+    {
+        const uint64_t P = static_cast<uint64_t>(t) * per_step;
+        if (u < m * kUnits) {
+            const uint64_t c = u / kUnits, g = u % kUnits;
+            const uint64_t base = P + c * 1024;
+            const uint64_t B = (base >> 2) + g;
+            const int i0 = static_cast<int>(4 * g) - static_cast<int>(base & 3);
+            uint32_t wr[4], wa[4];
+            gm.block(Ctr{{B + 1, 0, 0, 0}}, wr);
+            gm.block(Ctr{{B + 129, 0, 0, 0}}, wa);
+            const int lo = i0 < 0 ? -i0 : 0, hi = i0 + 4 > 512 ? 512 - i0 : 4;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (j >= lo && j < hi) {
+                    const uint64_t p0 = c * 1024 + static_cast<uint64_t>(i0 + j);
+                    pair(wr[j], wa[j], p0, p0 + 512, j);
+                }
+            }
+            *lo_out = lo;
+            *hi_out = hi;
+        } else {
+            const uint64_t i = u - m * kUnits, base = P + m * 1024;
+            WordCache wc{~0ull, {0, 0, 0, 0}};
+            const uint32_t wrad = word_at(gm, base + i, wc);
+            const uint32_t wang = word_at(gm, base + nu_tail + i, wc);
+            pair(wrad, wang, m * 1024 + i, m * 1024 + nu_tail + i, 0);
+            *lo_out = 0;
+            *hi_out = 1;
+        }
+    }
+
+    // the two words of the odd last particle (N odd)
+    __device__ __forceinline__ void odd_words(const PhiloxGen &gm, int t, uint32_t *w0, uint32_t *w1) const
+    {
+        const uint64_t P = static_cast<uint64_t>(t) * per_step;
+        WordCache wc{~0ull, {0, 0, 0, 0}};
+        *w0 = word_at(gm, P + N, wc);
+        *w1 = word_at(gm, P + N + 1, wc);
+    }
+};
+
+// What the backward pass needs of one replayed step (FP64 runs only).
+struct StepRecord {
+    double *x;       // particles after the move, before resampling [N]
+    double *l;       // log-weights [N]
+    uint32_t *rep;   // replication counts, when the step resampled [N]
+    uint32_t *sS;    // exclusive prefix of the surplus copies [N]
+    uint32_t *ep;    // empty slots in order [N]
+    uint8_t *flag;   // 1 when the step resampled
+};
+
+// Scalar state of a filter between steps (a checkpoint holds it together
+// with the particles and log-weights).
+struct FilterScalars {
+    double L_prev, ll_sum, Ls_prev, lls_sum, lshift, lshift_s;
+    uint64_t events;
+    int flat;
+};
+
+// One filter run by one CTA: state, and the step of the particle filter.
+//
+// SHADOW: every particle also carries an FP64 copy, propagated with the same
+// uniforms and the shadow parameters, weighted in FP64 and resampled with the
+// main run's decisions and parent indices.  With R = float and the same
+// parameters its log-likelihood isolates the FP32 arithmetic error from the
+// Monte Carlo divergence a flipped ancestor would otherwise start; with
+// R = double and perturbed parameters it is the common-random-numbers,
+// fixed-ancestor evaluation that finite differences of the estimate need.
 template <typename R, int THREADS, bool SHADOW>
-__global__ void __launch_bounds__(THREADS) k_pf_batched(const BatchedFilter *filt, const int *order, int nf,
+struct FilterRun {
+    NoiseLayout lay;
+    PhiloxGen gm, gr;
+    Step<R, SHADOW> st;
+    R *xc, *xn;
+    double *xsc, *xsn;
+    uint32_t *sS, *ep;
+    double threshold;
+    double L_prev, ll_sum, Ls_prev, lls_sum;
+    uint64_t events;
+
+    __device__ void setup(const BatchedFilter &F, R *xa, R *xb, R *lw, uint32_t *scanS, uint32_t *epos, double *xsa,
+        double *xsb, double *lws, double thr)
+    {
+        lay.init(F.n);
+        gm = PhiloxGen{F.mkey[0], F.mkey[1]};
+        gr = PhiloxGen{F.rkey[0], F.rkey[1]};
+        xc = xa + F.off;
+        xn = xb + F.off;
+        xsc = SHADOW ? xsa + F.off : nullptr;
+        xsn = SHADOW ? xsb + F.off : nullptr;
+        sS = scanS + F.off;
+        ep = epos + F.off;
+        threshold = thr;
+        st.l = lw + F.off;
+        st.ls = SHADOW ? lws + F.off : nullptr;
+        st.phi = static_cast<R>(F.phi);
+        st.sx = static_cast<R>(F.sx);
+        st.sd0 = static_cast<R>(F.sd0);
+        st.lconst = static_cast<R>(F.lconst);
+        st.hinv = static_cast<R>(F.hinv);
+        st.phi_d = F.phi_s;
+        st.sx_d = F.sx_s;
+        st.sd0_d = F.sd0_s;
+        st.lconst_d = F.lconst_s;
+        st.hinv_d = F.hinv_s;
+        st.lshift = 0;
+        st.lshift_s = 0.0;
+        st.flat = true;
+        L_prev = log(static_cast<double>(F.n));
+        ll_sum = 0.0;
+        Ls_prev = L_prev;
+        lls_sum = 0.0;
+        events = 0;
+    }
+
+    __device__ FilterScalars scalars() const
+    {
+        return FilterScalars{L_prev, ll_sum, Ls_prev, lls_sum, static_cast<double>(st.lshift), st.lshift_s, events,
+            st.flat ? 1 : 0};
+    }
+
+    __device__ void restore(const FilterScalars &c)
+    {
+        L_prev = c.L_prev;
+        ll_sum = c.ll_sum;
+        Ls_prev = c.Ls_prev;
+        lls_sum = c.lls_sum;
+        st.lshift = static_cast<R>(c.lshift);
+        st.lshift_s = c.lshift_s;
+        events = c.events;
+        st.flat = c.flat != 0;
+    }
+
+    // Step t: move, weight, normalise and (when ESS < N threshold) resample.
+    // `rec` (REC only) receives what the backward pass needs.
+    template <bool REC>
+    __device__ void step(int t, double yt_d, double *shd, R *shr, unsigned long long *shu, uint32_t *shj,
+        const StepRecord &rec)
+    {
+        const uint64_t N = lay.N;
+        st.x = xc;
+        st.xs = xsc;
+        st.init = (t == 0);
+        st.yt_d = yt_d;
+        st.yt = static_cast<R>(yt_d);
+        Lse<R> acc;
+        Lse<double> accs;
+        // ---- noise, propagation, log-weights, online normaliser
+        for (uint64_t u = threadIdx.x; u < lay.units; u += THREADS) {
+            R v[8];
+            double vs[8];
+            int lo, hi;
+            lay.unit(gm, t, u, &lo, &hi, [&](uint32_t wrad, uint32_t wang, uint64_t p0, uint64_t p1, int j) {
+                st.pair(wrad, wang, p0, p1, v + 2 * j, vs + 2 * j);
+            });
+            if (t > 0) {
+                acc.add(v, 2 * lo, 2 * hi);
+                if constexpr (SHADOW) accs.add(vs, 2 * lo, 2 * hi);
+            }
+        }
+        if ((N & 1) && threadIdx.x == THREADS - 1) {
+            uint32_t w0, w1;
+            lay.odd_words(gm, t, &w0, &w1);
+            R v[1];
+            double vs[1];
+            st.one(Math<R>::radius(u01oc<R>(w0)) * Math<R>::cos2pi(u01oc<R>(w1)), N - 1, v[0]);
+            if constexpr (SHADOW)
+                st.one_shadow(Math<double>::radius(u01oc<double>(w0)) * Math<double>::cos2pi(u01oc<double>(w1)),
+                    N - 1, vs[0]);
+            if (t > 0) {
+                acc.add(v, 0, 1);
+                if constexpr (SHADOW) accs.add(vs, 0, 1);
+            }
+        }
+        if (t == 0) {
+            __syncthreads();
+            return;
+        }
+        // ---- FP64 normaliser: S = sum exp(l - M), Q = sum exp^2; the log
+        // normaliser of the weights relative to M is carried to the next step,
+        // whose log-weights start from l - M
+        R M;
+        double S, Q;
+        block_lse(acc, shr, shd, &M, &S, &Q);
+        const double L = static_cast<double>(M) + log(S);
+        ll_sum += L - L_prev;
+        L_prev = log(S);
+        if constexpr (SHADOW) {
+            double Ms, Ss;
+            block_lse<double>(accs, shd, shd, &Ms, &Ss, nullptr);
+            lls_sum += Ms + log(Ss) - Ls_prev;
+            Ls_prev = log(Ss);
+            st.lshift_s = Ms;
+        }
+        st.lshift = M;
+        st.flat = false;
+        if constexpr (REC) {
+            for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
+                rec.x[p] = static_cast<double>(xc[p]);
+                rec.l[p] = static_cast<double>(st.l[p]);
+            }
+        }
+        const double ess = S * S / Q;
+        const bool resample = ess < static_cast<double>(N) * threshold;
+        if constexpr (REC) {
+            if (threadIdx.x == 0) *rec.flag = resample ? 1 : 0;
+        }
+        if (!resample) return;
+        // ---- systematic resampling
+        ++events;
+        uint32_t wr[2];
+        {
+            WordCache wc{~0ull, {0, 0, 0, 0}};
+            const uint64_t a = 2 * (events - 1);
+            wr[0] = word_at(gr, a, wc);
+            wr[1] = word_at(gr, a + 1, wc);
+        }
+        const double U = __dadd_rn(__dmul_rn(static_cast<double>(wr[0]), 0x1p-64),
+            __dmul_rn(static_cast<double>(wr[1]), 0x1p-32));
+        const double delta = 1.0 / static_cast<double>(N);
+        const double ud = U * delta;
+        const double invS = 1.0 / S;
+        // per tile of THREADS particles: inclusive FP64 scan of the
+        // normalised weights, cumulative counts j_p = #{k : u_k < c_p} (the
+        // lower bound of c_p on the grid fma(k, delta, ud)), the replication
+        // counts j_p - j_{p-1}, and the exclusive scan of (empty slot,
+        // surplus copies) that places the parents
+        double carry = 0.0;
+        unsigned long long carry2 = 0;
+        uint32_t jprev = 0;
+        for (uint64_t b = 0; b < N; b += THREADS) {
+            const uint64_t p = b + threadIdx.x;
+            const double w = p < N ? static_cast<double>(Math<R>::exp(st.l[p] - M)) * invS : 0.0;
+            double tot;
+            const double c = carry + block_inclusive_sum(w, shd, &tot);
+            carry += tot;
+            uint32_t jp = static_cast<uint32_t>(N);
+            if (p + 1 < N) {
+                double jf = ceil((c - ud) * static_cast<double>(N));
+                long long j = jf < 0 ? 0 : (jf > static_cast<double>(N) ? static_cast<long long>(N) : static_cast<long long>(jf));
+                while (j > 0 && fma(static_cast<double>(j - 1), delta, ud) >= c) --j;
+                while (j < static_cast<long long>(N) && fma(static_cast<double>(j), delta, ud) < c) ++j;
+                jp = static_cast<uint32_t>(j);
+            }
+            shj[threadIdx.x + 1] = jp;
+            if (threadIdx.x == 0) shj[0] = jprev;
+            __syncthreads();
+            const uint32_t rep = p < N ? shj[threadIdx.x + 1] - shj[threadIdx.x] : 0u;
+            jprev = shj[THREADS];
+            const unsigned long long v = p < N ? ((rep == 0 ? 1ull : 0ull) | (static_cast<unsigned long long>(rep > 0 ? rep - 1 : 0) << 32)) : 0ull;
+            unsigned long long tot2;
+            const unsigned long long inc = block_inclusive_sum(v, shu, &tot2);
+            const unsigned long long ex = carry2 + inc - v;
+            carry2 += tot2;
+            if (p < N) {
+                sS[p] = static_cast<uint32_t>(ex >> 32);
+                if constexpr (REC) {
+                    rec.rep[p] = rep;
+                    rec.sS[p] = static_cast<uint32_t>(ex >> 32);
+                }
+                if (rep == 0) {
+                    ep[ex & 0xffffffffull] = static_cast<uint32_t>(p);
+                } else {
+                    xn[p] = xc[p];  // occupied slots keep their particle
+                    if constexpr (SHADOW) xsn[p] = xsc[p];
+                }
+            }
+        }
+        __syncthreads();
+        const uint64_t n_empty = carry2 & 0xffffffffull;
+        for (uint64_t k = threadIdx.x; k < n_empty; k += THREADS) {
+            uint64_t lo = 0, hi = N;  // last source with surplus prefix <= k
+            while (hi - lo > 1) {
+                const uint64_t mid = (lo + hi) >> 1;
+                if (sS[mid] <= k) {
+                    lo = mid;
+                } else {
+                    hi = mid;
+                }
+            }
+            const uint32_t e = ep[k];
+            xn[e] = xc[lo];
+            if constexpr (SHADOW) xsn[e] = xsc[lo];
+            if constexpr (REC) rec.ep[k] = e;
+        }
+        __syncthreads();
+        // the gathered particles become the current ones, with equal weights
+        R *tx = xc;
+        xc = xn;
+        xn = tx;
+        if constexpr (SHADOW) {
+            double *ts = xsc;
+            xsc = xsn;
+            xsn = ts;
+        }
+        st.flat = true;
+        L_prev = log(static_cast<double>(N));
+        Ls_prev = L_prev;
+    }
+};
+
+template <typename R, int THREADS, bool SHADOW, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) k_pf_batched(const BatchedFilter *filt, const int *order, int nf,
     const double *y, int T, double threshold, R *xa, R *xb, R *lw, uint32_t *scanS, uint32_t *epos,
     double *loglik, uint32_t *nresampled, int *queue, double *xsa, double *xsb, double *lws,
     double *loglik_shadow)
@@ -217,7 +532,81 @@ __global__ void __launch_bounds__(THREADS) k_pf_batched(const BatchedFilter *fil
     __shared__ unsigned long long shu[33];
     __shared__ uint32_t shj[THREADS + 1];
     __shared__ int sh_f;
-    constexpr uint64_t kUnits = 129;  // units per full chunk
+    while (true) {
+        if (threadIdx.x == 0) {
+            const int k = atomicAdd(queue, 1);
+            sh_f = k < nf ? order[k] : -1;
+        }
+        __syncthreads();
+        const int f = sh_f;
+        __syncthreads();
+        if (f < 0) break;
+        FilterRun<R, THREADS, SHADOW> run;
+        run.setup(filt[f], xa, xb, lw, scanS, epos, xsa, xsb, lws, threshold);
+        const double *yf = y + static_cast<uint64_t>(f) * (T + 1);
+        for (int t = 0; t <= T; ++t) run.template step<false>(t, yf[t], shd, shr, shu, shj, StepRecord{});
+        if (threadIdx.x == 0) {
+            loglik[f] = run.ll_sum;
+            nresampled[f] = static_cast<uint32_t>(run.events);
+            if constexpr (SHADOW) loglik_shadow[f] = run.lls_sum;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint: gradient of the FP64 log-likelihood estimate with respect to
+// (phi, sx, sy), ancestors and resampling times held fixed.
+//
+// With the resampling steps r_1 < r_2 < ... fixed, the estimate is
+//   logL = sum over segments of [log sum_i exp(l_i at the segment's end) - log N],
+// l_i the sum of log g(y_t | x_t^i) over the segment, and x_t^j = phi
+// x~_{t-1}^j + sx eps_t^j, x~ the (possibly resampled) particles,
+// x_0 = sd0 eps_0 with sd0 = sx / sqrt(1 - phi^2).  Reverse mode, t = T..0,
+// with lambda_t = d logL / d x_t and w the softmax of l at the end of the
+// segment containing t:
+//   mu_t^i     = sum over children j of i of lambda_{t+1}^j  (gather; fixed ancestors)
+//   lambda_t^i = phi mu_t^i + w^i (y_t - x_t^i) / sy^2
+//   d/dphi  += sum_i x_t^i mu_t^i,   d/dsx += sum_j lambda_t^j eps_t^j,
+//   d/dsy   += sum_i w^i (-1/sy + (y_t - x_t^i)^2 / sy^3),
+// and at t = 0 the sd0 terms.  The forward pass keeps a checkpoint (particles,
+// log-weights, scalars) every C steps; the backward pass replays each block
+// of C steps from its checkpoint with the same kernel code -- same counters,
+// so the same noise, decisions and ancestors -- recording the particles and
+// the parent placement, then sweeps the block backwards.  The noise eps_t is
+// recomputed from the counters again in the sweep.  Nothing of size T x N is
+// stored.
+// ---------------------------------------------------------------------------
+struct AdjointArgs {
+    int C;                 // checkpoint interval (steps)
+    uint64_t total;        // particles over all filters (checkpoint stride)
+    double *ck_x, *ck_l;   // checkpoint k of filter f: [k * total + off, + n)
+    FilterScalars *ck_s;   // [k * F + f]
+    int F;
+    // per-CTA work areas, each for nmax particles
+    uint64_t nmax;
+    double *rec_x, *rec_l; // C x nmax per CTA
+    uint32_t *rec_rep, *rec_sS, *rec_ep;
+    uint8_t *rec_flag;     // C per CTA
+    double *lam, *mu, *wend;  // nmax per CTA
+    double *grad;          // 3 per filter
+};
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 1) k_pf_adjoint(const BatchedFilter *filt, const int *order, int nf,
+    const double *y, int T, double threshold, double *xa, double *xb, double *lw, uint32_t *scanS, uint32_t *epos,
+    double *loglik, uint32_t *nresampled, int *queue, AdjointArgs A)
+{
+    __shared__ double shd[33];
+    __shared__ unsigned long long shu[33];
+    __shared__ uint32_t shj[THREADS + 1];
+    __shared__ int sh_f;
+    const int C = A.C;
+    const uint64_t slot = blockIdx.x, cn = static_cast<uint64_t>(C) * A.nmax;
+    double *rx = A.rec_x + slot * cn, *rl = A.rec_l + slot * cn;
+    uint32_t *rrep = A.rec_rep + slot * cn, *rsS = A.rec_sS + slot * cn, *rep_list = A.rec_ep + slot * cn;
+    uint8_t *rflag = A.rec_flag + slot * C;
+    double *lam = A.lam + slot * A.nmax, *mu = A.mu + slot * A.nmax, *wend = A.wend + slot * A.nmax;
     while (true) {
         if (threadIdx.x == 0) {
             const int k = atomicAdd(queue, 1);
@@ -229,257 +618,243 @@ __global__ void __launch_bounds__(THREADS) k_pf_batched(const BatchedFilter *fil
         if (f < 0) break;
         const BatchedFilter F = filt[f];
         const uint64_t N = F.n;
-        R *xc = xa + F.off, *xn = xb + F.off;
-        double *xsc = SHADOW ? xsa + F.off : nullptr, *xsn = SHADOW ? xsb + F.off : nullptr;
-        uint32_t *sS = scanS + F.off, *ep = epos + F.off;
-        const PhiloxGen gm{F.mkey[0], F.mkey[1]}, gr{F.rkey[0], F.rkey[1]};
-        const uint64_t per_step = N + (N & 1) * 2;  // words of one normal_distribution(N) call
-        const uint64_t m = N / 1024, tail = N % 1024, nu_tail = tail / 2;
-        const uint64_t units = m * kUnits + nu_tail;
-        Step<R, SHADOW> st;
-        st.l = lw + F.off;
-        st.ls = SHADOW ? lws + F.off : nullptr;
-        st.phi = static_cast<R>(F.phi);
-        st.sx = static_cast<R>(F.sx);
-        st.sd0 = static_cast<R>(F.sd0);
-        st.lconst = static_cast<R>(F.lconst);
-        st.hinv = static_cast<R>(F.hinv);
-        st.phi_d = F.phi;
-        st.sx_d = F.sx;
-        st.sd0_d = F.sd0;
-        st.lconst_d = F.lconst;
-        st.hinv_d = F.hinv;
-        st.lshift = 0;
-        st.lshift_s = 0.0;
-        st.flat = true;
-        double L_prev = log(static_cast<double>(N)), ll_sum = 0.0;
-        double Ls_prev = L_prev, lls_sum = 0.0;
-        uint64_t events = 0;
+        const double *yf = y + static_cast<uint64_t>(f) * (T + 1);
+        const double phi = F.phi, sx = F.sx, sy = F.sy;
+        const double sy2inv = 1.0 / (sy * sy);
+        FilterRun<double, THREADS, false> run;
+        run.setup(F, xa, xb, lw, scanS, epos, nullptr, nullptr, nullptr, threshold);
+        auto save = [&](int k) {
+            double *cx = A.ck_x + static_cast<uint64_t>(k) * A.total + F.off;
+            double *cl = A.ck_l + static_cast<uint64_t>(k) * A.total + F.off;
+            for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
+                cx[p] = run.xc[p];
+                cl[p] = run.st.l[p];
+            }
+            if (threadIdx.x == 0) A.ck_s[static_cast<uint64_t>(k) * A.F + f] = run.scalars();
+            __syncthreads();  // the next step overwrites the particles
+        };
+        // ---- forward pass; checkpoints of the state after steps 0, C, 2C, ...
         for (int t = 0; t <= T; ++t) {
-            const uint64_t P = static_cast<uint64_t>(t) * per_step;
-            st.x = xc;
-            st.xs = xsc;
-            st.init = (t == 0);
-            st.yt_d = y[static_cast<uint64_t>(f) * (T + 1) + t];
-            st.yt = static_cast<R>(st.yt_d);
-            Lse<R> acc;
-            Lse<double> accs;
-            // ---- noise, propagation, log-weights, online normaliser
-            for (uint64_t u = threadIdx.x; u < units; u += THREADS) {
-                R v[8];
-                double vs[8];
-                if (u < m * kUnits) {
-                    const uint64_t c = u / kUnits, g = u % kUnits;
-                    const uint64_t base = P + c * 1024;
-                    const uint64_t B = (base >> 2) + g;
-                    const int i0 = static_cast<int>(4 * g) - static_cast<int>(base & 3);
-                    uint32_t wr[4], wa[4];
-                    gm.block(Ctr{{B + 1, 0, 0, 0}}, wr);
-                    gm.block(Ctr{{B + 129, 0, 0, 0}}, wa);
-                    const int lo = i0 < 0 ? -i0 : 0, hi = i0 + 4 > 512 ? 512 - i0 : 4;
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        if (j >= lo && j < hi) {
-                            const uint64_t p0 = c * 1024 + static_cast<uint64_t>(i0 + j);
-                            st.pair(wr[j], wa[j], p0, p0 + 512, v + 2 * j, vs + 2 * j);
-                        }
-                    }
-                    if (t > 0) {
-                        acc.add(v, 2 * lo, 2 * hi);
-                        if constexpr (SHADOW) accs.add(vs, 2 * lo, 2 * hi);
-                    }
-                } else {
-                    const uint64_t i = u - m * kUnits, base = P + m * 1024;
-                    WordCache wc{~0ull, {0, 0, 0, 0}};
-                    const uint32_t wrad = word_at(gm, base + i, wc);
-                    const uint32_t wang = word_at(gm, base + nu_tail + i, wc);
-                    st.pair(wrad, wang, m * 1024 + i, m * 1024 + nu_tail + i, v, vs);
-                    if (t > 0) {
-                        acc.add(v, 0, 2);
-                        if constexpr (SHADOW) accs.add(vs, 0, 2);
-                    }
-                }
-            }
-            if ((N & 1) && threadIdx.x == THREADS - 1) {
-                // odd N: the last particle from the two words after the chunks
-                WordCache wc{~0ull, {0, 0, 0, 0}};
-                const uint32_t w0 = word_at(gm, P + N, wc), w1 = word_at(gm, P + N + 1, wc);
-                R v[1];
-                double vs[1];
-                st.one(Math<R>::radius(u01oc<R>(w0)) * Math<R>::cos2pi(u01oc<R>(w1)), N - 1, v[0]);
-                if constexpr (SHADOW)
-                    st.one_shadow(Math<double>::radius(u01oc<double>(w0)) * Math<double>::cos2pi(u01oc<double>(w1)),
-                        N - 1, vs[0]);
-                if (t > 0) {
-                    acc.add(v, 0, 1);
-                    if constexpr (SHADOW) accs.add(vs, 0, 1);
-                }
-            }
-            if (t == 0) {
-                __syncthreads();
-                continue;
-            }
-            // ---- FP64 normaliser: S = sum exp(l - M), Q = sum exp^2; the
-            // log normaliser of the weights relative to M is carried to the
-            // next step, whose log-weights start from l - M
-            R M;
-            double S, Q;
-            block_lse(acc, shr, shd, &M, &S, &Q);
-            const double L = static_cast<double>(M) + log(S);
-            ll_sum += L - L_prev;
-            L_prev = log(S);
-            if constexpr (SHADOW) {
-                double Ms, Ss;
-                block_lse<double>(accs, shd, shd, &Ms, &Ss, nullptr);
-                lls_sum += Ms + log(Ss) - Ls_prev;
-                Ls_prev = log(Ss);
-                st.lshift_s = Ms;
-            }
-            st.lshift = M;
-            st.flat = false;
-            const double ess = S * S / Q;
-            if (!(ess < static_cast<double>(N) * threshold)) continue;
-            // ---- systematic resampling
-            ++events;
-            uint32_t wr[2];
-            {
-                WordCache wc{~0ull, {0, 0, 0, 0}};
-                const uint64_t a = 2 * (events - 1);
-                wr[0] = word_at(gr, a, wc);
-                wr[1] = word_at(gr, a + 1, wc);
-            }
-            const double U = __dadd_rn(__dmul_rn(static_cast<double>(wr[0]), 0x1p-64),
-                __dmul_rn(static_cast<double>(wr[1]), 0x1p-32));
-            const double delta = 1.0 / static_cast<double>(N);
-            const double ud = U * delta;
-            const double invS = 1.0 / S;
-            // per tile of THREADS particles: inclusive FP64 scan of the
-            // normalised weights, cumulative counts j_p = #{k : u_k < c_p}
-            // (the lower bound of c_p on the grid fma(k, delta, ud)), the
-            // replication counts j_p - j_{p-1}, and the exclusive scan of
-            // (empty slot, surplus copies) that places the parents
-            double carry = 0.0;
-            unsigned long long carry2 = 0;
-            uint32_t jprev = 0;
-            for (uint64_t b = 0; b < N; b += THREADS) {
-                const uint64_t p = b + threadIdx.x;
-                const double w = p < N ? static_cast<double>(Math<R>::exp(st.l[p] - M)) * invS : 0.0;
-                double tot;
-                const double c = carry + block_inclusive_sum(w, shd, &tot);
-                carry += tot;
-                uint32_t jp = static_cast<uint32_t>(N);
-                if (p + 1 < N) {
-                    double jf = ceil((c - ud) * static_cast<double>(N));
-                    long long j = jf < 0 ? 0 : (jf > static_cast<double>(N) ? static_cast<long long>(N) : static_cast<long long>(jf));
-                    while (j > 0 && fma(static_cast<double>(j - 1), delta, ud) >= c) --j;
-                    while (j < static_cast<long long>(N) && fma(static_cast<double>(j), delta, ud) < c) ++j;
-                    jp = static_cast<uint32_t>(j);
-                }
-                shj[threadIdx.x + 1] = jp;
-                if (threadIdx.x == 0) shj[0] = jprev;
-                __syncthreads();
-                const uint32_t rep = p < N ? shj[threadIdx.x + 1] - shj[threadIdx.x] : 0u;
-                jprev = shj[THREADS];
-                const unsigned long long v = p < N ? ((rep == 0 ? 1ull : 0ull) | (static_cast<unsigned long long>(rep > 0 ? rep - 1 : 0) << 32)) : 0ull;
-                unsigned long long tot2;
-                const unsigned long long inc = block_inclusive_sum(v, shu, &tot2);
-                const unsigned long long ex = carry2 + inc - v;
-                carry2 += tot2;
-                if (p < N) {
-                    sS[p] = static_cast<uint32_t>(ex >> 32);
-                    if (rep == 0) {
-                        ep[ex & 0xffffffffull] = static_cast<uint32_t>(p);
-                    } else {
-                        xn[p] = xc[p];  // occupied slots keep their particle
-                        if constexpr (SHADOW) xsn[p] = xsc[p];
-                    }
-                }
-            }
-            __syncthreads();
-            const uint64_t n_empty = carry2 & 0xffffffffull;
-            for (uint64_t k = threadIdx.x; k < n_empty; k += THREADS) {
-                uint64_t lo = 0, hi = N;  // last source with surplus prefix <= k
-                while (hi - lo > 1) {
-                    const uint64_t mid = (lo + hi) >> 1;
-                    if (sS[mid] <= k) {
-                        lo = mid;
-                    } else {
-                        hi = mid;
-                    }
-                }
-                xn[ep[k]] = xc[lo];
-                if constexpr (SHADOW) xsn[ep[k]] = xsc[lo];
-            }
-            __syncthreads();
-            // the gathered particles become the current ones, with equal weights
-            R *tx = xc;
-            xc = xn;
-            xn = tx;
-            if constexpr (SHADOW) {
-                double *ts = xsc;
-                xsc = xsn;
-                xsn = ts;
-            }
-            st.flat = true;
-            L_prev = log(static_cast<double>(N));
-            Ls_prev = L_prev;
+            run.template step<false>(t, yf[t], shd, shd, shu, shj, StepRecord{});
+            if (t % C == 0) save(t / C);
         }
         if (threadIdx.x == 0) {
-            loglik[f] = ll_sum;
-            nresampled[f] = static_cast<uint32_t>(events);
-            if constexpr (SHADOW) loglik_shadow[f] = lls_sum;
+            loglik[f] = run.ll_sum;
+            nresampled[f] = static_cast<uint32_t>(run.events);
+        }
+        __syncthreads();
+        // ---- backward pass
+        double g_phi = 0.0, g_sx = 0.0, g_sy = 0.0;
+        for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
+            lam[p] = 0.0;
+            wend[p] = 0.0;
+        }
+        __syncthreads();
+        // noise of step t paired with lambda: sum_j lambda_j eps_j
+        auto lam_eps = [&](int t) {
+            double acc = 0.0;
+            for (uint64_t u = threadIdx.x; u < run.lay.units; u += THREADS) {
+                int lo, hi;
+                run.lay.unit(run.gm, t, u, &lo, &hi, [&](uint32_t wrad, uint32_t wang, uint64_t p0, uint64_t p1, int) {
+                    const double r = Math<double>::radius(u01oc<double>(wrad));
+                    double sn, cs;
+                    Math<double>::sincos2pi(u01oc<double>(wang), &sn, &cs);
+                    acc += lam[p0] * (r * sn) + lam[p1] * (r * cs);
+                });
+            }
+            if ((N & 1) && threadIdx.x == THREADS - 1) {
+                uint32_t w0, w1;
+                run.lay.odd_words(run.gm, t, &w0, &w1);
+                acc += lam[N - 1] * (Math<double>::radius(u01oc<double>(w0)) * Math<double>::cos2pi(u01oc<double>(w1)));
+            }
+            return acc;
+        };
+        const int nblk = T / C;  // blocks (kC, min(kC + C, T)], k = 0 .. nblk
+        for (int k = nblk; k >= 0; --k) {
+            const int t0 = k * C, t1 = min(t0 + C, T);
+            if (t1 <= t0) continue;
+            // replay steps t0+1 .. t1 from checkpoint k, recording them
+            {
+                const double *cx = A.ck_x + static_cast<uint64_t>(k) * A.total + F.off;
+                const double *cl = A.ck_l + static_cast<uint64_t>(k) * A.total + F.off;
+                run.setup(F, xa, xb, lw, scanS, epos, nullptr, nullptr, nullptr, threshold);
+                for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
+                    run.xc[p] = cx[p];
+                    run.st.l[p] = cl[p];
+                }
+                run.restore(A.ck_s[static_cast<uint64_t>(k) * A.F + f]);
+                __syncthreads();
+            }
+            for (int t = t0 + 1; t <= t1; ++t) {
+                const uint64_t q = static_cast<uint64_t>(t - t0 - 1);
+                const StepRecord rec{rx + q * A.nmax, rl + q * A.nmax, rrep + q * A.nmax, rsS + q * A.nmax,
+                    rep_list + q * A.nmax, rflag + q};
+                run.template step<true>(t, yf[t], shd, shd, shu, shj, rec);
+            }
+            __syncthreads();
+            // sweep t1 .. t0+1
+            for (int t = t1; t >= t0 + 1; --t) {
+                const uint64_t q = static_cast<uint64_t>(t - t0 - 1);
+                const double *xt = rx + q * A.nmax, *lt = rl + q * A.nmax;
+                const bool res = rflag[q] != 0;
+                // mu_t: children sums of lambda_{t+1} (zero past the last step)
+                if (t < T) {
+                    const uint32_t *rp = rrep + q * A.nmax, *ss = rsS + q * A.nmax, *el = rep_list + q * A.nmax;
+                    for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
+                        double m_ = lam[p];
+                        if (res) {
+                            const uint32_t r = rp[p];
+                            m_ = r ? lam[p] : 0.0;
+                            for (uint32_t c = 1; c < r; ++c) m_ += lam[el[ss[p] + c - 1]];
+                        }
+                        mu[p] = m_;
+                        g_phi += xt[p] * m_;
+                    }
+                } else {
+                    for (uint64_t p = threadIdx.x; p < N; p += THREADS) mu[p] = 0.0;
+                }
+                // weights at the end of the segment containing t
+                if (t == T || res) {
+                    double mx = -INFINITY;
+                    for (uint64_t p = threadIdx.x; p < N; p += THREADS) mx = fmax(mx, lt[p]);
+                    mx = block_max(mx, shd);
+                    double ssum = 0.0;
+                    for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
+                        const double e = exp(lt[p] - mx);
+                        wend[p] = e;
+                        ssum += e;
+                    }
+                    ssum = block_sum(ssum, shd);
+                    const double inv = 1.0 / ssum;
+                    for (uint64_t p = threadIdx.x; p < N; p += THREADS) wend[p] *= inv;
+                }
+                __syncthreads();
+                const double yt = yf[t];
+                for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
+                    const double r = yt - xt[p];
+                    lam[p] = phi * mu[p] + wend[p] * r * sy2inv;
+                    g_sy += wend[p] * (r * r * sy2inv / sy - 1.0 / sy);
+                }
+                __syncthreads();
+                g_sx += lam_eps(t);
+                __syncthreads();
+            }
+        }
+        // ---- t = 0: x_0 = sd0 eps_0, no weight; mu_0 = lambda_1 (no resampling at t = 0)
+        {
+            const double *cx = A.ck_x + F.off;  // checkpoint 0: the particles of step 0
+            for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
+                g_phi += cx[p] * lam[p];
+                lam[p] = phi * lam[p];
+            }
+            __syncthreads();
+            const double le = lam_eps(0);
+            const double q = 1.0 - phi * phi;
+            g_sx += le / sqrt(q);
+            g_phi += le * sx * phi / (q * sqrt(q));
+        }
+        g_phi = block_sum(g_phi, shd);
+        g_sx = block_sum(g_sx, shd);
+        g_sy = block_sum(g_sy, shd);
+        if (threadIdx.x == 0) {
+            A.grad[3 * f] = g_phi;
+            A.grad[3 * f + 1] = g_sx;
+            A.grad[3 * f + 2] = g_sy;
         }
         __syncthreads();
     }
 }
 
-template <typename R, int THREADS, bool SHADOW>
+// Two register budgets per block shape: MINB = 1 (the compiler's choice, 16
+// warps per SM at most) and MINB = 1024 / THREADS (64 registers, 32 warps).
+template <typename R, int THREADS, bool SHADOW, int MINB>
 int launch_one(const BatchedArgs &a, const int *order, int nf, int *queue, int ctas, cudaStream_t s)
 {
-    k_pf_batched<R, THREADS, SHADOW><<<ctas, THREADS, 0, s>>>(a.filt, order, nf, a.y, a.T, a.threshold,
+    k_pf_batched<R, THREADS, SHADOW, MINB><<<ctas, THREADS, 0, s>>>(a.filt, order, nf, a.y, a.T, a.threshold,
         static_cast<R *>(a.xa), static_cast<R *>(a.xb), static_cast<R *>(a.lw), a.scanS, a.epos,
         a.loglik, a.nresampled, queue, a.xsa, a.xsb, a.lws, a.loglik_shadow);
     MB_LAUNCH_CHECK();
     return MCKL_B200_OK;
 }
 
-template <typename R, int THREADS, bool SHADOW>
+template <typename R, int THREADS, bool SHADOW, int MINB>
 int occupancy_one(int *blocks)
 {
-    MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, k_pf_batched<R, THREADS, SHADOW>, THREADS, 0));
+    MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, k_pf_batched<R, THREADS, SHADOW, MINB>, THREADS,
+        0));
     return MCKL_B200_OK;
 }
 
-template <typename R, bool SHADOW>
-int occupancy_threads(int threads, int *blocks)
+// op 0: launch, op 1: occupancy of the variant
+template <typename R, int THREADS, bool SHADOW>
+int variant(int op, bool capped, const BatchedArgs &a, const int *order, int nf, int *queue, int ctas,
+    cudaStream_t s, int *blocks)
 {
-    switch (threads) {
-        case 128: return occupancy_one<R, 128, SHADOW>(blocks);
-        case 256: return occupancy_one<R, 256, SHADOW>(blocks);
-        case 512: return occupancy_one<R, 512, SHADOW>(blocks);
-        default: return occupancy_one<R, 1024, SHADOW>(blocks);
-    }
+    constexpr int CAP = 1024 / THREADS;
+    if (op == 1) return capped ? occupancy_one<R, THREADS, SHADOW, CAP>(blocks) : occupancy_one<R, THREADS, SHADOW, 1>(blocks);
+    return capped ? launch_one<R, THREADS, SHADOW, CAP>(a, order, nf, queue, ctas, s)
+                  : launch_one<R, THREADS, SHADOW, 1>(a, order, nf, queue, ctas, s);
 }
 
 template <typename R, bool SHADOW>
-int launch_threads(const BatchedArgs &a, const int *order, int nf, int threads, int *queue, int ctas, cudaStream_t s)
+int dispatch_threads(int op, int threads, bool capped, const BatchedArgs &a, const int *order, int nf, int *queue,
+    int ctas, cudaStream_t s, int *blocks)
 {
     switch (threads) {
-        case 128: return launch_one<R, 128, SHADOW>(a, order, nf, queue, ctas, s);
-        case 256: return launch_one<R, 256, SHADOW>(a, order, nf, queue, ctas, s);
-        case 512: return launch_one<R, 512, SHADOW>(a, order, nf, queue, ctas, s);
-        default: return launch_one<R, 1024, SHADOW>(a, order, nf, queue, ctas, s);
+        case 128: return variant<R, 128, SHADOW>(op, capped, a, order, nf, queue, ctas, s, blocks);
+        case 256: return variant<R, 256, SHADOW>(op, capped, a, order, nf, queue, ctas, s, blocks);
+        case 512: return variant<R, 512, SHADOW>(op, capped, a, order, nf, queue, ctas, s, blocks);
+        default: return variant<R, 1024, SHADOW>(op, capped, a, order, nf, queue, ctas, s, blocks);
     }
+}
+
+int dispatch(int op, int threads, bool capped, const BatchedArgs &a, const int *order, int nf, int *queue, int ctas,
+    cudaStream_t s, int *blocks)
+{
+    if (a.fp64 && a.xsa) return dispatch_threads<double, true>(op, threads, capped, a, order, nf, queue, ctas, s, blocks);
+    if (a.fp64) return dispatch_threads<double, false>(op, threads, capped, a, order, nf, queue, ctas, s, blocks);
+    if (a.xsa) return dispatch_threads<float, true>(op, threads, capped, a, order, nf, queue, ctas, s, blocks);
+    return dispatch_threads<float, false>(op, threads, capped, a, order, nf, queue, ctas, s, blocks);
 }
 
 }  // namespace
 
-// resident CTAs per SM of the kernel variant the arguments select
-int pf_batched_occupancy(const BatchedArgs &a, int threads, int *blocks)
+// Resident CTAs per SM of the kernel variant that the arguments and block
+// shape select, and whether that variant is the register-capped one: the
+// uncapped variant when it fits `ctas_per_sm`, else the capped one.
+int pf_batched_fit(const BatchedArgs &a, int threads, int ctas_per_sm, bool *capped, int *fit)
 {
-    if (a.fp64) return occupancy_threads<double, false>(threads, blocks);
-    if (a.xsa) return occupancy_threads<float, true>(threads, blocks);
-    return occupancy_threads<float, false>(threads, blocks);
+    int f0 = 0, f1 = 0;
+    int rc = dispatch(1, threads, false, a, nullptr, 0, nullptr, 0, nullptr, &f0);
+    if (rc != MCKL_B200_OK) return rc;
+    rc = dispatch(1, threads, true, a, nullptr, 0, nullptr, 0, nullptr, &f1);
+    if (rc != MCKL_B200_OK) return rc;
+    *capped = f0 < ctas_per_sm;
+    *fit = *capped ? f1 : f0;
+    return MCKL_B200_OK;
+}
+
+template <int THREADS>
+int adjoint_one(const BatchedArgs &a, const int *order, int nf, int *queue, const AdjointArgs &A, int ctas,
+    cudaStream_t s)
+{
+    k_pf_adjoint<THREADS><<<ctas, THREADS, 0, s>>>(a.filt, order, nf, a.y, a.T, a.threshold,
+        static_cast<double *>(a.xa), static_cast<double *>(a.xb), static_cast<double *>(a.lw), a.scanS, a.epos,
+        a.loglik, a.nresampled, queue, A);
+    MB_LAUNCH_CHECK();
+    return MCKL_B200_OK;
+}
+
+int pf_adjoint_launch(const BatchedArgs &a, const int *order, int nf, int threads, int *queue, const AdjointArgs &A,
+    int ctas, cudaStream_t s)
+{
+    MB_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), s));
+    switch (threads) {
+        case 128: return adjoint_one<128>(a, order, nf, queue, A, ctas, s);
+        case 256: return adjoint_one<256>(a, order, nf, queue, A, ctas, s);
+        case 512: return adjoint_one<512>(a, order, nf, queue, A, ctas, s);
+        default: return adjoint_one<1024>(a, order, nf, queue, A, ctas, s);
+    }
 }
 
 int pf_batched_launch(const BatchedArgs &a, const int *order, int nf, int threads, int ctas_per_sm, int *queue,
@@ -488,11 +863,13 @@ int pf_batched_launch(const BatchedArgs &a, const int *order, int nf, int thread
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    bool capped = false;
+    int fit = 0;
+    int rc = pf_batched_fit(a, threads, ctas_per_sm, &capped, &fit);
+    if (rc != MCKL_B200_OK) return rc;
     const int ctas = std::max(1, std::min(nf, sms * ctas_per_sm));
     MB_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), s));
-    if (a.fp64) return launch_threads<double, false>(a, order, nf, threads, queue, ctas, s);
-    if (a.xsa) return launch_threads<float, true>(a, order, nf, threads, queue, ctas, s);
-    return launch_threads<float, false>(a, order, nf, threads, queue, ctas, s);
+    return dispatch(0, threads, capped, a, order, nf, queue, ctas, s, nullptr);
 }
 
 }  // namespace mckl_b200
@@ -512,9 +889,27 @@ struct mckl_b200_batched {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaStream_t graph_stream = nullptr;
+    std::vector<mckl_b200::BatchedFilter> hf;  // host copy of the filter table
+    uint64_t nmax = 0;                         // largest particle count
+    void *adj_mem = nullptr;                   // adjoint checkpoints and work areas
+    size_t adj_bytes = 0;
 };
 
 using namespace mckl_b200;
+
+namespace {
+
+// shadow-run parameters of one filter (the same derived constants as the main run's)
+void set_shadow(BatchedFilter &h, double phi, double sx, double sy)
+{
+    h.phi_s = phi;
+    h.sx_s = sx;
+    h.sd0_s = sx / std::sqrt(1 - phi * phi);
+    h.lconst_s = -std::log(sy) - 0.5 * std::log(2 * 3.14159265358979323846);
+    h.hinv_s = 0.5 / (sy * sy);
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -536,6 +931,8 @@ int mckl_b200_batched_create(mckl_b200_batched_t **out, size_t F, const size_t *
         h[f].sd0 = sx[f] / std::sqrt(1 - phi[f] * phi[f]);
         h[f].lconst = -std::log(sy[f]) - 0.5 * std::log(2 * 3.14159265358979323846);
         h[f].hinv = 0.5 / (sy[f] * sy[f]);
+        h[f].sy = sy[f];
+        set_shadow(h[f], phi[f], sx[f], sy[f]);
         h[f].mkey[0] = mkeys[2 * f];
         h[f].mkey[1] = mkeys[2 * f + 1];
         h[f].rkey[0] = rkeys[2 * f];
@@ -551,8 +948,9 @@ int mckl_b200_batched_create(mckl_b200_batched_t **out, size_t F, const size_t *
     b->T = static_cast<int>(T);
     b->total = total;
     b->threshold = threshold;
-    const bool shadow = (fp64 == 2);
-    b->fp64 = (fp64 == 1) ? 1 : 0;
+    MB_CHECK_ARG(fp64 >= 0 && fp64 <= 3, "fp64: 0 FP32, 1 FP64, 2 FP32 + FP64 shadow, 3 FP64 + FP64 shadow");
+    const bool shadow = (fp64 >= 2);
+    b->fp64 = (fp64 == 1 || fp64 == 3) ? 1 : 0;
     const size_t rs = b->fp64 ? 8 : 4;
     const size_t bytes = align256(F * sizeof(BatchedFilter)) + align256(F * (T + 1) * 8) + 3 * align256(total * rs) +
                          2 * align256(total * 4) + align256(F * 8) + align256(F * 4) + align256(F * 4) + 256 +
@@ -591,6 +989,8 @@ int mckl_b200_batched_create(mckl_b200_batched_t **out, size_t F, const size_t *
     MB_CUDA(cudaMemcpy(b->a.filt, h.data(), F * sizeof(BatchedFilter), cudaMemcpyHostToDevice));
     MB_CUDA(cudaMemcpy(b->a.y, y, F * (T + 1) * 8, cudaMemcpyHostToDevice));
     MB_CUDA(cudaMemcpy(b->order, order.data(), F * 4, cudaMemcpyHostToDevice));
+    b->hf = h;
+    for (size_t f = 0; f < F; ++f) b->nmax = std::max<uint64_t>(b->nmax, N[f]);
     *out = b;
     return MCKL_B200_OK;
 }
@@ -646,10 +1046,10 @@ int mckl_b200_batched_autotune(mckl_b200_batched_t *b, int max_trials, int *thre
 {
     MB_CHECK_ARG(b != nullptr && max_trials >= 0, "bad arguments");
     cudaStream_t s = as_stream(stream);
-    // candidate block shapes: 4 to 8 warps per scheduler in total, from many
-    // small CTAs (small filters keep every thread busy) to few large ones
-    // (fewer barriers per particle on the large filters)
-    static const int cand[][2] = {{128, 8}, {128, 12}, {256, 4}, {256, 6}, {512, 2}, {512, 3}, {1024, 1}, {1024, 2}};
+    // candidate block shapes: 16 or 32 resident warps per SM (the latter with
+    // the register-capped variant), from many small CTAs (small filters keep
+    // every thread busy) to few large ones (fewer barriers per particle)
+    static const int cand[][2] = {{128, 4}, {128, 8}, {256, 2}, {256, 4}, {512, 1}, {512, 2}, {1024, 1}};
     int best = -1, n = 0;
     float best_ms = 0.0f;
     cudaEvent_t e0, e1;
@@ -659,7 +1059,8 @@ int mckl_b200_batched_autotune(mckl_b200_batched_t *b, int max_trials, int *thre
     int rc = pf_batched_launch(b->a, b->order, b->F, 256, 4, b->queue, s);
     for (int k = 0; rc == MCKL_B200_OK && k < static_cast<int>(sizeof(cand) / sizeof(cand[0])); ++k) {
         int fit = 0;
-        rc = pf_batched_occupancy(b->a, cand[k][0], &fit);
+        bool capped = false;
+        rc = pf_batched_fit(b->a, cand[k][0], cand[k][1], &capped, &fit);
         if (rc != MCKL_B200_OK) break;
         if (fit < cand[k][1]) continue;  // would not be resident at once
         cudaEventRecord(e0, s);
@@ -720,9 +1121,83 @@ int mckl_b200_batched_results(mckl_b200_batched_t *b, double *loglik, uint32_t *
     return MCKL_B200_OK;
 }
 
+int mckl_b200_batched_shadow_params(mckl_b200_batched_t *b, const double *phi, const double *sx, const double *sy)
+{
+    MB_CHECK_ARG(b != nullptr && phi && sx && sy, "null argument");
+    MB_CHECK_ARG(b->a.xsa != nullptr, "the handle has no shadow run (fp64 = 2 or 3)");
+    for (int f = 0; f < b->F; ++f) {
+        MB_CHECK_ARG(sy[f] > 0 && phi[f] * phi[f] < 1, "need sy > 0 and |phi| < 1");
+        set_shadow(b->hf[f], phi[f], sx[f], sy[f]);
+    }
+    MB_CUDA(cudaMemcpy(b->a.filt, b->hf.data(), b->hf.size() * sizeof(BatchedFilter), cudaMemcpyHostToDevice));
+    return MCKL_B200_OK;
+}
+
+int mckl_b200_batched_adjoint(mckl_b200_batched_t *b, int checkpoint_every, double *loglik, double *grad,
+    void *stream)
+{
+    MB_CHECK_ARG(b != nullptr && grad != nullptr, "null argument");
+    MB_CHECK_ARG(b->fp64 == 1 && b->a.xsa == nullptr, "the adjoint needs a handle created with fp64 = 1");
+    MB_CHECK_ARG(checkpoint_every >= 1 && checkpoint_every <= 4096, "checkpoint_every in [1, 4096]");
+    cudaStream_t s = as_stream(stream);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int ctas = std::max(1, std::min(b->F, sms));
+    const uint64_t C = static_cast<uint64_t>(checkpoint_every);
+    const uint64_t nck = static_cast<uint64_t>(b->T) / C + 1;
+    const uint64_t nm = b->nmax;
+    // checkpoints + per-CTA replay records + per-CTA adjoint vectors + gradients
+    const size_t need = 2 * align256(nck * b->total * 8) + align256(nck * b->F * sizeof(FilterScalars)) +
+                        2 * align256(ctas * C * nm * 8) + 3 * align256(ctas * C * nm * 4) + align256(ctas * C) +
+                        3 * align256(ctas * nm * 8) + align256(static_cast<size_t>(b->F) * 24);
+    if (b->adj_bytes < need) {
+        if (b->adj_mem) cudaFree(b->adj_mem);
+        b->adj_mem = nullptr;
+        b->adj_bytes = 0;
+        if (cudaMalloc(&b->adj_mem, need) != cudaSuccess) {
+            set_error("adjoint work memory (" + std::to_string(need >> 20) + " MiB) could not be allocated; "
+                      "use a larger checkpoint interval or fewer filters per handle");
+            return MCKL_B200_ERR_NOMEM;
+        }
+        b->adj_bytes = need;
+    }
+    char *p = static_cast<char *>(b->adj_mem);
+    auto take = [&p](size_t n) {
+        char *q = p;
+        p += align256(n);
+        return q;
+    };
+    AdjointArgs A{};
+    A.C = checkpoint_every;
+    A.total = b->total;
+    A.F = b->F;
+    A.nmax = nm;
+    A.ck_x = reinterpret_cast<double *>(take(nck * b->total * 8));
+    A.ck_l = reinterpret_cast<double *>(take(nck * b->total * 8));
+    A.ck_s = reinterpret_cast<FilterScalars *>(take(nck * b->F * sizeof(FilterScalars)));
+    A.rec_x = reinterpret_cast<double *>(take(ctas * C * nm * 8));
+    A.rec_l = reinterpret_cast<double *>(take(ctas * C * nm * 8));
+    A.rec_rep = reinterpret_cast<uint32_t *>(take(ctas * C * nm * 4));
+    A.rec_sS = reinterpret_cast<uint32_t *>(take(ctas * C * nm * 4));
+    A.rec_ep = reinterpret_cast<uint32_t *>(take(ctas * C * nm * 4));
+    A.rec_flag = reinterpret_cast<uint8_t *>(take(ctas * C));
+    A.lam = reinterpret_cast<double *>(take(ctas * nm * 8));
+    A.mu = reinterpret_cast<double *>(take(ctas * nm * 8));
+    A.wend = reinterpret_cast<double *>(take(ctas * nm * 8));
+    A.grad = reinterpret_cast<double *>(take(static_cast<size_t>(b->F) * 24));
+    int rc = pf_adjoint_launch(b->a, b->order, b->F, b->threads, b->queue, A, ctas, s);
+    if (rc != MCKL_B200_OK) return rc;
+    if (loglik) MB_CUDA(cudaMemcpyAsync(loglik, b->a.loglik, b->F * 8, cudaMemcpyDeviceToHost, s));
+    MB_CUDA(cudaMemcpyAsync(grad, A.grad, static_cast<size_t>(b->F) * 24, cudaMemcpyDeviceToHost, s));
+    MB_CUDA(cudaStreamSynchronize(s));
+    return MCKL_B200_OK;
+}
+
 int mckl_b200_batched_destroy(mckl_b200_batched_t *b)
 {
     if (!b) return MCKL_B200_OK;
+    if (b->adj_mem) cudaFree(b->adj_mem);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     if (b->mem) cudaFree(b->mem);

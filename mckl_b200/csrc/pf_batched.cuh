@@ -10,7 +10,9 @@ namespace mckl_b200 {
 struct BatchedFilter {
     uint64_t n;         // particles
     uint64_t off;       // offset of this filter's particles in the work arrays
-    double phi, sx, sd0, lconst, hinv;
+    double phi, sx, sd0, lconst, hinv, sy;
+    // shadow run (FP64, follows the main run's decisions): its parameters
+    double phi_s, sx_s, sd0_s, lconst_s, hinv_s;
     uint32_t mkey[2];   // model stream: Philox4x32 key
     uint32_t rkey[2];   // resampling stream: Philox4x32 key
 };
