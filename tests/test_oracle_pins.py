@@ -163,3 +163,20 @@ def test_oracle_vs_compiled_reference_randomized(orc):
             alpha = float(rng.uniform(0.1, 12))
             assert same_bits(orc.gamma(a, f64, n2, alpha, 0.7), ref.gamma(b, f64, n2, alpha, 0.7))
             assert a.state() == b.state()
+
+
+def test_kalman_gradient_vs_finite_differences(orc):
+    """The Kalman oracle's forward-mode gradient against central differences."""
+    e = O.Engine.make(1, key=(7,))
+    for (phi, sx, sy) in ((0.9, 1.0, 0.5), (0.55, 1.7, 0.25), (0.97, 0.6, 0.9)):
+        y = np.concatenate([[0.0], np.cumsum(orc.normal(e, True, 200, 0.0, 1.0)) * 0.1])
+        _, g = orc.kalman_ar1(y, phi, sx, sy)
+        h = 1e-6
+        for k in range(3):
+            p = [phi, sx, sy]
+            p[k] += h
+            lp, _ = orc.kalman_ar1(y, *p)
+            p[k] -= 2 * h
+            lm, _ = orc.kalman_ar1(y, *p)
+            fd = (lp - lm) / (2 * h)
+            assert abs(fd - g[k]) <= 1e-6 * max(1.0, abs(fd)), (k, fd, g[k])
