@@ -23,6 +23,10 @@ flush is needed.  Also measured in the same run (rank 0):
     logL_FP64 the FP64 shadow run along the same genealogy (same counters,
     same ancestors; target 1e-6), and the estimates' offset from the exact
     Kalman log-likelihood;
+  * `adjoint`: the differentiated configuration -- gradients of the FP64
+    estimates in (phi, sx, sy) for 256 parameter sets, N = 2^16, T = 1000,
+    ancestors fixed, against central finite differences under common random
+    numbers and against the Kalman gradient;
   * `rng`: the RNG + distributions configuration (see below), one step.
 
 Workload `rng`: for each of Threefry4x64-20 and ARS-5, seeded 42, 2^28 values
@@ -273,6 +277,52 @@ def bench_smc(args, rank, world, dev):
         extra["ratio_vs_plain"] = value / world / extra["plain_gpu"]["particle_steps_per_s"]
     out["extra"] = extra
     return out
+
+
+def bench_adjoint(rank, dev, sets=256, N=1 << 16, T=1000, C=32, threads=512):
+    """Differentiated SMC: gradient of the FP64 estimate in (phi, sx, sy) for
+    `sets` parameter sets drawn like the batched workload, N particles, T
+    observations, ancestors fixed and replayed from the counters."""
+    import numpy as np
+    import torch
+
+    import mckl_b200 as mb
+    import oracle as O
+    from mckl_b200 import autograd as AG
+
+    w = mb.batched_workload(F=sets, T=T, seed=4321 + 7919 * rank, nmin=N, nmax=N + 1)
+    b = mb.BatchedFilters(w["N"], w["y"], w["phi"], w["sx"], w["sy"], w["mkeys"], w["rkeys"], fp64=True)
+    b.config(threads, 1)
+    b.adjoint(C)  # warm-up (allocates the checkpoint and replay memory)
+    stream = torch.cuda.current_stream()
+    t0, t1 = events()
+    t0.record(stream)
+    ll, g = b.adjoint(C)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    b.close()
+    w["threads"] = threads
+    fd = AG.finite_differences(w, h=1e-5, threads=threads)
+    rel_fd = np.abs(g - fd) / np.maximum(np.abs(fd), 1.0)
+    orc = O.CPUPath("oracle")
+    kg = np.zeros_like(g)
+    kll = np.zeros(sets)
+    for f in range(sets):
+        kll[f], kg[f] = orc.kalman_ar1(w["y"][f], w["phi"][f], w["sx"][f], w["sy"][f])
+    rel_k = np.linalg.norm(g - kg, axis=1) / np.linalg.norm(kg, axis=1)
+    cos = np.sum(g * kg, axis=1) / (np.linalg.norm(g, axis=1) * np.linalg.norm(kg, axis=1))
+    ps = float(sets) * N * T
+    return {"workload": f"{sets} parameter sets, N = {N}, T = {T}, FP64, checkpoint every {C} steps, "
+                        f"{threads} threads per filter",
+            "ms": ms, "forward_particle_steps_per_s": ps / (ms / 1e3),
+            "vs_fd_rel": {"max": float(rel_fd.max()), "median": float(np.median(rel_fd)),
+                          "frac_le_1e-4": float(np.mean(rel_fd <= 1e-4)),
+                          "definition": "|adjoint - central FD (h = 1e-5, common random numbers, base ancestors)| "
+                                        "/ max(|FD|, 1)"},
+            "vs_kalman": {"rel_norm_median": float(np.median(rel_k)), "cosine_median": float(np.median(cos)),
+                          "loglik_minus_kalman_mean": float(np.mean(ll - kll)),
+                          "note": "fixed ancestors: a biased estimate of the exact score at any N"}}
 
 
 # ---------------------------------------------------------------------------
@@ -594,6 +644,8 @@ def main():
         }
         line.update(res.get("extra", {}))
         if args.parts == "all":
+            if rank == 0:
+                line["adjoint"] = bench_adjoint(rank, dev)
             rng = bench_rng(rank, world, dev, steps=1, warmup=1, e2e=False, clocks_on=False)
             ph = rng["philox_c1"]["rand_u32_2^26"]["GB_s"]
             line["rng"] = {"value_GB_s": rng["value"],

@@ -12,8 +12,9 @@
 // therefore depend on the previous chunks: the chunks of one stream run in
 // order.  A CTA owns one stream and processes each chunk with all its
 // threads: the chunk's words are staged in shared memory, every thread
-// transforms K / THREADS values, the N redraws are replayed by one thread in
-// index order, and the accepted values are compacted with a CTA-wide rank.
+// transforms K / THREADS values, the N redraws are assigned in index order by
+// one warp (the scalar normals they consume form one sequence, evaluated 64 at
+// a time), and the accepted values are compacted with a CTA-wide rank.
 // Independent streams (gamma_blocks: one stream per block of samples, each on
 // its own counter range) run one per CTA across the GPU.
 //
@@ -413,20 +414,55 @@ __device__ uint32_t gamma_chunk(const G &g, const GammaParam<R> &k, const Ctr &B
         }
         if (nred) {
             __syncthreads();
-            if (threadIdx.x == 0) {
+            if (threadIdx.x < 32) {
+                // The scalar normals after the batch words form one sequence
+                // z_0, z_1, ... (pair j: words 2j, 2j + 1; z_2j = r cos, z_2j+1
+                // = r sin, the second returned from the cache); the q-th
+                // redrawn element takes the q-th z with 1 + c z > 0.  A warp
+                // evaluates 64 z at a time and assigns them by ballot ranks.
+                const int lane = threadIdx.x;
+                const unsigned lt = (1u << lane) - 1u;
                 ScalarWords<G, W> sw{&g, B, off};
-                uint64_t sp = pos + nw;
-                ScalarNormal<R> rn;
-                for (uint32_t q = 0; q < nred; ++q) {
-                    R wz, vz;
-                    do {
-                        wz = rn(sw, sp);
-                        vz = O::add(static_cast<R>(1), O::mul(c, wz));
-                    } while (vz <= 0);
-                    lw[q] = wz;
-                    lv[q] = vz;
+                const uint64_t sp0 = pos + nw;
+                uint32_t done = 0;
+                uint64_t used = 0;  // normals consumed
+                for (uint64_t pb = 0; done < nred; pb += 32) {
+                    const uint64_t j = pb + lane;
+                    uint64_t k = sp0 + 2 * j;
+                    ScalarNormal<R> rn;
+                    const R z0 = rn(sw, k), z1 = rn(sw, k);
+                    const R v0 = O::add(static_cast<R>(1), O::mul(c, z0));
+                    const R v1 = O::add(static_cast<R>(1), O::mul(c, z1));
+                    const bool a0 = v0 > 0, a1 = v1 > 0;
+                    const unsigned m0 = __ballot_sync(0xffffffffu, a0), m1 = __ballot_sync(0xffffffffu, a1);
+                    const uint32_t before = __popc(m0 & lt) + __popc(m1 & lt);
+                    const uint32_t r0 = before, r1 = before + (a0 ? 1u : 0u);
+                    const uint32_t need = nred - done;
+                    if (a0 && r0 < need) {
+                        lw[done + r0] = z0;
+                        lv[done + r0] = v0;
+                    }
+                    if (a1 && r1 < need) {
+                        lw[done + r1] = z1;
+                        lv[done + r1] = v1;
+                    }
+                    const uint32_t tot = __popc(m0) + __popc(m1);
+                    if (tot >= need) {
+                        // the need-th accepted normal is the last one consumed
+                        const bool last0 = a0 && r0 == need - 1, last1 = a1 && r1 == need - 1;
+                        const unsigned ml = __ballot_sync(0xffffffffu, last0 || last1);
+                        const int src = __ffs(ml) - 1;
+                        const uint32_t idx = last0 ? 2u * lane : 2u * lane + 1u;
+                        const uint32_t li = __shfl_sync(0xffffffffu, idx, src);
+                        used = 2 * pb + li + 1;
+                        done = nred;
+                    } else {
+                        done += tot;
+                    }
                 }
-                *sh_pos = sp - (pos + nw);
+                // consumed words: two per started pair (a cached second value
+                // is dropped with the chunk's normal generator)
+                if (lane == 0) *sh_pos = 2 * ((used + 1) / 2);
             }
             __syncthreads();
 #pragma unroll
@@ -498,7 +534,7 @@ __device__ uint32_t gamma_chunk(const G &g, const GammaParam<R> &k, const Ctr &B
 // when `blocks` is set, else at the engine state given (one stream), whose
 // final state goes to *state_out.
 template <class G, typename W, typename R, int THREADS>
-__global__ void __launch_bounds__(THREADS) k_gamma(G g, Ctr ctr0, uint32_t idx0, int blocks, uint64_t nstreams,
+__global__ void __launch_bounds__(THREADS, 3) k_gamma(G g, Ctr ctr0, uint32_t idx0, int blocks, uint64_t nstreams,
     uint64_t n, const GammaParam<R> *params, R *r, Ctr *ctr_out, uint32_t *idx_out)
 {
     using S = GammaSmem<G, W, R>;

@@ -62,6 +62,10 @@ struct Math<float> {
     __device__ static void sincos2pi(float v, float *s, float *c) { sincospif(2.0f * v, s, c); }
     __device__ static float cos2pi(float v) { return cospif(2.0f * v); }
     __device__ static float exp(float a) { return expf(a); }
+    __device__ static float mul(float a, float b) { return __fmul_rn(a, b); }
+    __device__ static float add(float a, float b) { return __fadd_rn(a, b); }
+    __device__ static float sub(float a, float b) { return __fsub_rn(a, b); }
+    __device__ static float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 };
 
 template <>
@@ -70,6 +74,10 @@ struct Math<double> {
     __device__ static void sincos2pi(double v, double *s, double *c) { sincospi(2.0 * v, s, c); }
     __device__ static double cos2pi(double v) { return cospi(2.0 * v); }
     __device__ static double exp(double a) { return ::exp(a); }
+    __device__ static double mul(double a, double b) { return __dmul_rn(a, b); }
+    __device__ static double add(double a, double b) { return __dadd_rn(a, b); }
+    __device__ static double sub(double a, double b) { return __dsub_rn(a, b); }
+    __device__ static double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
 };
 
 template <typename T>
@@ -109,16 +117,16 @@ struct Lse {
             if (k >= lo && k < hi) gm = fmax(gm, v[k]);
         if (gm > m) {
             const double sc = (m == -INFINITY) ? 0.0 : ::exp(static_cast<double>(m) - static_cast<double>(gm));
-            s *= sc;
-            q *= sc * sc;
+            s = __dmul_rn(s, sc);
+            q = __dmul_rn(q, __dmul_rn(sc, sc));
             m = gm;
         }
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             if (k >= lo && k < hi) {
-                const double e = static_cast<double>(Math<R>::exp(v[k] - m));
-                s += e;
-                q += e * e;
+                const double e = static_cast<double>(Math<R>::exp(Math<R>::sub(v[k], m)));
+                s = __dadd_rn(s, e);
+                q = __fma_rn(e, e, q);
             }
         }
     }
@@ -131,8 +139,8 @@ __device__ __forceinline__ void block_lse(const Lse<R> &a, R *shr, double *shd, 
     const R mm = block_max(a.m, shr);
     const double sc = (a.m == -INFINITY) ? 0.0 : ::exp(static_cast<double>(a.m) - static_cast<double>(mm));
     *M = mm;
-    *S = block_sum(a.s * sc, shd);
-    if (Q) *Q = block_sum(a.q * sc * sc, shd);
+    *S = block_sum(__dmul_rn(a.s, sc), shd);
+    if (Q) *Q = block_sum(__dmul_rn(a.q, __dmul_rn(sc, sc)), shd);
 }
 
 // One Box-Muller pair of one filter at step t: the noise from a radius and an
@@ -153,42 +161,44 @@ struct Step {
         const R rr = Math<R>::radius(u01oc<R>(wrad));
         R sn, cs;
         Math<R>::sincos2pi(u01oc<R>(wang), &sn, &cs);
-        one(rr * sn, p0, v[0]);
-        one(rr * cs, p1, v[1]);
+        one(Math<R>::mul(rr, sn), p0, v[0]);
+        one(Math<R>::mul(rr, cs), p1, v[1]);
         if constexpr (SHADOW) {
             const double rd = Math<double>::radius(u01oc<double>(wrad));
             double snd, csd;
             Math<double>::sincos2pi(u01oc<double>(wang), &snd, &csd);
-            one_shadow(rd * snd, p0, vs[0]);
-            one_shadow(rd * csd, p1, vs[1]);
+            one_shadow(__dmul_rn(rd, snd), p0, vs[0]);
+            one_shadow(__dmul_rn(rd, csd), p1, vs[1]);
         }
     }
 
     __device__ __forceinline__ void one(R e, uint64_t p, R &v) const
     {
+        using O = Math<R>;
         if (init) {
-            x[p] = sd0 * e;
+            x[p] = O::mul(sd0, e);
             return;
         }
-        const R xn = phi * x[p] + sx * e;
+        const R xn = O::fma(phi, x[p], O::mul(sx, e));
         x[p] = xn;
-        const R r = yt - xn;
-        const R lo = flat ? R(0) : l[p] - lshift;
-        v = lo + (lconst - r * r * hinv);
+        const R r = O::sub(yt, xn);
+        const R lo = flat ? R(0) : O::sub(l[p], lshift);
+        v = O::add(lo, O::fma(-O::mul(r, r), hinv, lconst));
         l[p] = v;
     }
 
     __device__ __forceinline__ void one_shadow(double e, uint64_t p, double &v) const
     {
+        using O = Math<double>;
         if (init) {
-            xs[p] = sd0_d * e;
+            xs[p] = O::mul(sd0_d, e);
             return;
         }
-        const double xn = phi_d * xs[p] + sx_d * e;
+        const double xn = O::fma(phi_d, xs[p], O::mul(sx_d, e));
         xs[p] = xn;
-        const double r = yt_d - xn;
-        const double lo = flat ? 0.0 : ls[p] - lshift_s;
-        v = lo + (lconst_d - r * r * hinv_d);
+        const double r = O::sub(yt_d, xn);
+        const double lo = flat ? 0.0 : O::sub(ls[p], lshift_s);
+        v = O::add(lo, O::fma(-O::mul(r, r), hinv_d, lconst_d));
         ls[p] = v;
     }
 };
@@ -261,16 +271,6 @@ struct NoiseLayout {
     }
 };
 
-// What the backward pass needs of one replayed step (FP64 runs only).
-struct StepRecord {
-    double *x;       // particles after the move, before resampling [N]
-    double *l;       // log-weights [N]
-    uint32_t *rep;   // replication counts, when the step resampled [N]
-    uint32_t *sS;    // exclusive prefix of the surplus copies [N]
-    uint32_t *ep;    // empty slots in order [N]
-    uint8_t *flag;   // 1 when the step resampled
-};
-
 // Scalar state of a filter between steps (a checkpoint holds it together
 // with the particles and log-weights).
 struct FilterScalars {
@@ -298,7 +298,7 @@ struct FilterRun {
     uint32_t *sS, *ep;
     double threshold;
     double L_prev, ll_sum, Ls_prev, lls_sum;
-    uint64_t events;
+    uint64_t events, n_empty;
 
     __device__ void setup(const BatchedFilter &F, R *xa, R *xb, R *lw, uint32_t *scanS, uint32_t *epos, double *xsa,
         double *xsb, double *lws, double thr)
@@ -353,11 +353,10 @@ struct FilterRun {
         st.flat = c.flat != 0;
     }
 
-    // Step t: move, weight, normalise and (when ESS < N threshold) resample.
-    // `rec` (REC only) receives what the backward pass needs.
-    template <bool REC>
-    __device__ void step(int t, double yt_d, double *shd, R *shr, unsigned long long *shu, uint32_t *shj,
-        const StepRecord &rec)
+    // Step t: move, weight, normalise and (when ESS < N threshold) resample;
+    // returns whether it resampled.  After a resampling the particles before
+    // it are still in xn, the placement in sS / ep[0, n_empty).
+    __device__ bool step(int t, double yt_d, double *shd, R *shr, unsigned long long *shu, uint32_t *shj)
     {
         const uint64_t N = lay.N;
         st.x = xc;
@@ -385,9 +384,9 @@ struct FilterRun {
             lay.odd_words(gm, t, &w0, &w1);
             R v[1];
             double vs[1];
-            st.one(Math<R>::radius(u01oc<R>(w0)) * Math<R>::cos2pi(u01oc<R>(w1)), N - 1, v[0]);
+            st.one(Math<R>::mul(Math<R>::radius(u01oc<R>(w0)), Math<R>::cos2pi(u01oc<R>(w1))), N - 1, v[0]);
             if constexpr (SHADOW)
-                st.one_shadow(Math<double>::radius(u01oc<double>(w0)) * Math<double>::cos2pi(u01oc<double>(w1)),
+                st.one_shadow(__dmul_rn(Math<double>::radius(u01oc<double>(w0)), Math<double>::cos2pi(u01oc<double>(w1))),
                     N - 1, vs[0]);
             if (t > 0) {
                 acc.add(v, 0, 1);
@@ -396,7 +395,7 @@ struct FilterRun {
         }
         if (t == 0) {
             __syncthreads();
-            return;
+            return false;
         }
         // ---- FP64 normaliser: S = sum exp(l - M), Q = sum exp^2; the log
         // normaliser of the weights relative to M is carried to the next step,
@@ -416,18 +415,8 @@ struct FilterRun {
         }
         st.lshift = M;
         st.flat = false;
-        if constexpr (REC) {
-            for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
-                rec.x[p] = static_cast<double>(xc[p]);
-                rec.l[p] = static_cast<double>(st.l[p]);
-            }
-        }
         const double ess = S * S / Q;
-        const bool resample = ess < static_cast<double>(N) * threshold;
-        if constexpr (REC) {
-            if (threadIdx.x == 0) *rec.flag = resample ? 1 : 0;
-        }
-        if (!resample) return;
+        if (!(ess < static_cast<double>(N) * threshold)) return false;
         // ---- systematic resampling
         ++events;
         uint32_t wr[2];
@@ -476,10 +465,6 @@ struct FilterRun {
             carry2 += tot2;
             if (p < N) {
                 sS[p] = static_cast<uint32_t>(ex >> 32);
-                if constexpr (REC) {
-                    rec.rep[p] = rep;
-                    rec.sS[p] = static_cast<uint32_t>(ex >> 32);
-                }
                 if (rep == 0) {
                     ep[ex & 0xffffffffull] = static_cast<uint32_t>(p);
                 } else {
@@ -489,7 +474,7 @@ struct FilterRun {
             }
         }
         __syncthreads();
-        const uint64_t n_empty = carry2 & 0xffffffffull;
+        n_empty = carry2 & 0xffffffffull;
         for (uint64_t k = threadIdx.x; k < n_empty; k += THREADS) {
             uint64_t lo = 0, hi = N;  // last source with surplus prefix <= k
             while (hi - lo > 1) {
@@ -503,7 +488,6 @@ struct FilterRun {
             const uint32_t e = ep[k];
             xn[e] = xc[lo];
             if constexpr (SHADOW) xsn[e] = xsc[lo];
-            if constexpr (REC) rec.ep[k] = e;
         }
         __syncthreads();
         // the gathered particles become the current ones, with equal weights
@@ -518,6 +502,7 @@ struct FilterRun {
         st.flat = true;
         L_prev = log(static_cast<double>(N));
         Ls_prev = L_prev;
+        return true;
     }
 };
 
@@ -544,7 +529,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_pf_batched(const BatchedFilte
         FilterRun<R, THREADS, SHADOW> run;
         run.setup(filt[f], xa, xb, lw, scanS, epos, xsa, xsb, lws, threshold);
         const double *yf = y + static_cast<uint64_t>(f) * (T + 1);
-        for (int t = 0; t <= T; ++t) run.template step<false>(t, yf[t], shd, shr, shu, shj, StepRecord{});
+        for (int t = 0; t <= T; ++t) run.step(t, yf[t], shd, shr, shu, shj);
         if (threadIdx.x == 0) {
             loglik[f] = run.ll_sum;
             nresampled[f] = static_cast<uint32_t>(run.events);
@@ -588,6 +573,7 @@ struct AdjointArgs {
     double *rec_x, *rec_l; // C x nmax per CTA
     uint32_t *rec_rep, *rec_sS, *rec_ep;
     uint8_t *rec_flag;     // C per CTA
+    uint32_t *rec_ne;      // empty slots of each recorded resampling, C per CTA
     double *lam, *mu, *wend;  // nmax per CTA
     double *grad;          // 3 per filter
 };
@@ -606,6 +592,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_adjoint(const BatchedFilter *
     double *rx = A.rec_x + slot * cn, *rl = A.rec_l + slot * cn;
     uint32_t *rrep = A.rec_rep + slot * cn, *rsS = A.rec_sS + slot * cn, *rep_list = A.rec_ep + slot * cn;
     uint8_t *rflag = A.rec_flag + slot * C;
+    uint32_t *rne = A.rec_ne + slot * C;
     double *lam = A.lam + slot * A.nmax, *mu = A.mu + slot * A.nmax, *wend = A.wend + slot * A.nmax;
     while (true) {
         if (threadIdx.x == 0) {
@@ -635,7 +622,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_adjoint(const BatchedFilter *
         };
         // ---- forward pass; checkpoints of the state after steps 0, C, 2C, ...
         for (int t = 0; t <= T; ++t) {
-            run.template step<false>(t, yf[t], shd, shd, shu, shj, StepRecord{});
+            run.step(t, yf[t], shd, shd, shu, shj);
             if (t % C == 0) save(t / C);
         }
         if (threadIdx.x == 0) {
@@ -659,13 +646,13 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_adjoint(const BatchedFilter *
                     const double r = Math<double>::radius(u01oc<double>(wrad));
                     double sn, cs;
                     Math<double>::sincos2pi(u01oc<double>(wang), &sn, &cs);
-                    acc += lam[p0] * (r * sn) + lam[p1] * (r * cs);
+                    acc += lam[p0] * __dmul_rn(r, sn) + lam[p1] * __dmul_rn(r, cs);
                 });
             }
             if ((N & 1) && threadIdx.x == THREADS - 1) {
                 uint32_t w0, w1;
                 run.lay.odd_words(run.gm, t, &w0, &w1);
-                acc += lam[N - 1] * (Math<double>::radius(u01oc<double>(w0)) * Math<double>::cos2pi(u01oc<double>(w1)));
+                acc += lam[N - 1] * __dmul_rn(Math<double>::radius(u01oc<double>(w0)), Math<double>::cos2pi(u01oc<double>(w1)));
             }
             return acc;
         };
@@ -687,11 +674,34 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_adjoint(const BatchedFilter *
             }
             for (int t = t0 + 1; t <= t1; ++t) {
                 const uint64_t q = static_cast<uint64_t>(t - t0 - 1);
-                const StepRecord rec{rx + q * A.nmax, rl + q * A.nmax, rrep + q * A.nmax, rsS + q * A.nmax,
-                    rep_list + q * A.nmax, rflag + q};
-                run.template step<true>(t, yf[t], shd, shd, shu, shj, rec);
+                const bool res = run.step(t, yf[t], shd, shd, shu, shj);
+                // record: particles before any resampling, log-weights, and
+                // the parent placement (occupied flags, surplus prefix, empties)
+                const double *xpre = res ? run.xn : run.xc;
+                double *qx = rx + q * A.nmax, *ql = rl + q * A.nmax;
+                uint32_t *qo = rrep + q * A.nmax, *qs = rsS + q * A.nmax, *qe = rep_list + q * A.nmax;
+                for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
+                    qx[p] = xpre[p];
+                    ql[p] = run.st.l[p];
+                    if (res) {
+                        qo[p] = 1;
+                        qs[p] = run.sS[p];
+                    }
+                }
+                if (threadIdx.x == 0) {
+                    rflag[q] = res ? 1 : 0;
+                    rne[q] = res ? static_cast<uint32_t>(run.n_empty) : 0u;
+                }
+                __syncthreads();
+                if (res) {
+                    for (uint64_t k2 = threadIdx.x; k2 < run.n_empty; k2 += THREADS) {
+                        const uint32_t e = run.ep[k2];
+                        qe[k2] = e;
+                        qo[e] = 0;
+                    }
+                }
+                __syncthreads();
             }
-            __syncthreads();
             // sweep t1 .. t0+1
             for (int t = t1; t >= t0 + 1; --t) {
                 const uint64_t q = static_cast<uint64_t>(t - t0 - 1);
@@ -699,13 +709,16 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_adjoint(const BatchedFilter *
                 const bool res = rflag[q] != 0;
                 // mu_t: children sums of lambda_{t+1} (zero past the last step)
                 if (t < T) {
-                    const uint32_t *rp = rrep + q * A.nmax, *ss = rsS + q * A.nmax, *el = rep_list + q * A.nmax;
+                    // children of parent p: slot p itself when occupied, and
+                    // the empty slots el[ss[p], ss[p + 1]) it fills
+                    const uint32_t *occ = rrep + q * A.nmax, *ss = rsS + q * A.nmax, *el = rep_list + q * A.nmax;
+                    const uint32_t ne = rne[q];
                     for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
                         double m_ = lam[p];
                         if (res) {
-                            const uint32_t r = rp[p];
-                            m_ = r ? lam[p] : 0.0;
-                            for (uint32_t c = 1; c < r; ++c) m_ += lam[el[ss[p] + c - 1]];
+                            m_ = occ[p] ? lam[p] : 0.0;
+                            const uint32_t end = p + 1 < N ? ss[p + 1] : ne;
+                            for (uint32_t c = ss[p]; c < end; ++c) m_ += lam[el[c]];
                         }
                         mu[p] = m_;
                         g_phi += xt[p] * m_;
@@ -1149,7 +1162,7 @@ int mckl_b200_batched_adjoint(mckl_b200_batched_t *b, int checkpoint_every, doub
     const uint64_t nm = b->nmax;
     // checkpoints + per-CTA replay records + per-CTA adjoint vectors + gradients
     const size_t need = 2 * align256(nck * b->total * 8) + align256(nck * b->F * sizeof(FilterScalars)) +
-                        2 * align256(ctas * C * nm * 8) + 3 * align256(ctas * C * nm * 4) + align256(ctas * C) +
+                        2 * align256(ctas * C * nm * 8) + 3 * align256(ctas * C * nm * 4) + align256(ctas * C) + align256(ctas * C * 4) +
                         3 * align256(ctas * nm * 8) + align256(static_cast<size_t>(b->F) * 24);
     if (b->adj_bytes < need) {
         if (b->adj_mem) cudaFree(b->adj_mem);
@@ -1182,6 +1195,7 @@ int mckl_b200_batched_adjoint(mckl_b200_batched_t *b, int checkpoint_every, doub
     A.rec_sS = reinterpret_cast<uint32_t *>(take(ctas * C * nm * 4));
     A.rec_ep = reinterpret_cast<uint32_t *>(take(ctas * C * nm * 4));
     A.rec_flag = reinterpret_cast<uint8_t *>(take(ctas * C));
+    A.rec_ne = reinterpret_cast<uint32_t *>(take(ctas * C * 4));
     A.lam = reinterpret_cast<double *>(take(ctas * nm * 8));
     A.mu = reinterpret_cast<double *>(take(ctas * nm * 8));
     A.wend = reinterpret_cast<double *>(take(ctas * nm * 8));
