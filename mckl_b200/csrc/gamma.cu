@@ -294,7 +294,9 @@ struct GammaSmem {
     static constexpr int kStageBlocks = (2 * K + 2) / WPB + 2;
     static constexpr int kStageBytes = kStageBlocks * G::kWords * 4;
     static constexpr int kListBytes = K * (4 + 2 * static_cast<int>(sizeof(R)));
-    static constexpr int kBytes = kStageBytes > kListBytes ? kStageBytes : kListBytes;
+    static constexpr int kMainBytes = ((kStageBytes > kListBytes ? kStageBytes : kListBytes) + 15) / 16 * 16;
+    // plus the batch normals of algorithm N
+    static constexpr int kBytes = kMainBytes + K * static_cast<int>(sizeof(R));
 };
 
 // One chunk of n <= K values at stream word `pos`; accepted values go to
@@ -365,36 +367,39 @@ __device__ uint32_t gamma_chunk(const G &g, const GammaParam<R> &k, const Ctr &B
         }
         __syncthreads();
     } else {
-        // ---- algorithm N: u, the batch normals w, v = fma(c, w, 1)
-        R u[EPT], w[EPT], v[EPT];
+        // ---- algorithm N: the batch normals, one Box-Muller pair per thread
+        // and pass into shared memory, then per element u, w, v = fma(c, w, 1)
+        R *wbuf = reinterpret_cast<R *>(smem + S::kMainBytes);
         const uint32_t nu = n / 2;
         const uint64_t q0 = s0 + n;  // first normal word in the staging buffer
+        for (uint32_t p = threadIdx.x; p < nu; p += THREADS) {
+            const R u1 = RealOps<R>::u01(kOC, st[q0 + p]);
+            const R u2 = O::mul(O::kTwoPi, RealOps<R>::u01(kOC, st[q0 + nu + p]));
+            const R sr = O::sqrt(O::mul(static_cast<R>(-2), O::log(u1)));
+            R sn, cs;
+            O::sincos(u2, &sn, &cs);
+            wbuf[p] = O::mul(sr, sn);
+            wbuf[nu + p] = O::mul(sr, cs);
+        }
+        if ((n & 1u) && threadIdx.x == THREADS - 1) {
+            // odd n: the last normal from the two words after the batch
+            const R a = RealOps<R>::u01(kOC, st[q0 + n]);
+            const R b = RealOps<R>::u01(kOC, st[q0 + n + 1]);
+            const R sr = O::mul(static_cast<R>(1), O::sqrt(O::mul(static_cast<R>(-2), O::log(a))));
+            R sn, cs;
+            O::sincos(O::mul(O::kTwoPi, b), &sn, &cs);
+            wbuf[n - 1] = O::add(static_cast<R>(0), O::mul(sr, cs));
+        }
+        __syncthreads();
+        R u[EPT], w[EPT], v[EPT];
 #pragma unroll
         for (int j = 0; j < EPT; ++j) {
             const uint32_t i = threadIdx.x + j * THREADS;
             u[j] = w[j] = v[j] = 0;
             if (i >= n) continue;
             u[j] = RealOps<R>::u01(kOO, st[s0 + i]);
-            R z;
-            if (i < 2 * nu) {
-                const uint32_t p = i < nu ? i : i - nu;
-                const R u1 = RealOps<R>::u01(kOC, st[q0 + p]);
-                const R u2 = O::mul(O::kTwoPi, RealOps<R>::u01(kOC, st[q0 + nu + p]));
-                const R s = O::sqrt(O::mul(static_cast<R>(-2), O::log(u1)));
-                R sn, cs;
-                O::sincos(u2, &sn, &cs);
-                z = O::mul(s, i < nu ? sn : cs);
-            } else {
-                // odd n: the last normal from the two words after the batch
-                const R a = RealOps<R>::u01(kOC, st[q0 + n]);
-                const R b = RealOps<R>::u01(kOC, st[q0 + n + 1]);
-                const R s = O::mul(static_cast<R>(1), O::sqrt(O::mul(static_cast<R>(-2), O::log(a))));
-                R sn, cs;
-                O::sincos(O::mul(O::kTwoPi, b), &sn, &cs);
-                z = O::add(static_cast<R>(0), O::mul(s, cs));
-            }
-            w[j] = z;
-            v[j] = O::fma(c, z, static_cast<R>(1));
+            w[j] = wbuf[i];
+            v[j] = O::fma(c, w[j], static_cast<R>(1));
         }
         // ---- redraws of v <= 0, in index order, by one thread
         uint32_t *lidx = reinterpret_cast<uint32_t *>(smem);

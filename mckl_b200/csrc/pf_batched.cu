@@ -46,11 +46,18 @@ __device__ __forceinline__ uint32_t word_at(const PhiloxGen &g, uint64_t w, Word
     return c.w[w & 3];
 }
 
-// U01OC<double> of a word, rounded to the propagation type
+// U01OC<double> of a word, rounded to the propagation type: (w + 1) 2^-32 is
+// exact in double; in float it is RN(w + 1) 2^-32, one integer conversion
 template <typename R>
 __device__ __forceinline__ R u01oc(uint32_t w)
 {
     return static_cast<R>(__dadd_rn(__dmul_rn(static_cast<double>(w), 0x1p-32), 0x1p-32));
+}
+
+template <>
+__device__ __forceinline__ float u01oc<float>(uint32_t w)
+{
+    return w == 0xFFFFFFFFu ? 1.0f : __fmul_rn(__uint2float_rn(w + 1u), 0x1p-32f);
 }
 
 template <typename R>
@@ -432,41 +439,56 @@ struct FilterRun {
         const double ud = U * delta;
         const double invS = 1.0 / S;
         // per tile of THREADS particles: inclusive FP64 scan of the
-        // normalised weights, cumulative counts j_p = #{k : u_k < c_p} (the
-        // lower bound of c_p on the grid fma(k, delta, ud)), the replication
-        // counts j_p - j_{p-1}, and the exclusive scan of (empty slot,
-        // surplus copies) that places the parents
+        // normalised weights; cumulative counts j_p = #{k : u_k < c_p} (the
+        // lower bound of c_p on the grid fma(k, delta, ud)); replication
+        // counts rep_p = j_p - j_{p-1}; the empty slots (rep = 0) in order,
+        // ranked by a CTA ballot; and the surplus copies of the parents
+        // before p, sS_p = sum_{i<p} max(rep_i - 1, 0) = j_{p-1} - p + E_p
+        // with E_p the empty slots before p
+        constexpr int NW = THREADS / 32;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        uint32_t *shw = reinterpret_cast<uint32_t *>(shu);
+        const uint32_t N32 = static_cast<uint32_t>(N);
+        const double dN = static_cast<double>(N);
         double carry = 0.0;
-        unsigned long long carry2 = 0;
-        uint32_t jprev = 0;
-        for (uint64_t b = 0; b < N; b += THREADS) {
-            const uint64_t p = b + threadIdx.x;
-            const double w = p < N ? static_cast<double>(Math<R>::exp(st.l[p] - M)) * invS : 0.0;
+        uint32_t jprev = 0, ecarry = 0;
+        for (uint32_t b = 0; b < N32; b += THREADS) {
+            const uint32_t p = b + threadIdx.x;
+            const double w = p < N32 ? static_cast<double>(Math<R>::exp(Math<R>::sub(st.l[p], M))) * invS : 0.0;
             double tot;
             const double c = carry + block_inclusive_sum(w, shd, &tot);
             carry += tot;
-            uint32_t jp = static_cast<uint32_t>(N);
-            if (p + 1 < N) {
-                double jf = ceil((c - ud) * static_cast<double>(N));
-                long long j = jf < 0 ? 0 : (jf > static_cast<double>(N) ? static_cast<long long>(N) : static_cast<long long>(jf));
-                while (j > 0 && fma(static_cast<double>(j - 1), delta, ud) >= c) --j;
-                while (j < static_cast<long long>(N) && fma(static_cast<double>(j), delta, ud) < c) ++j;
-                jp = static_cast<uint32_t>(j);
+            int jp = static_cast<int>(N32);
+            if (p + 1 < N32) {
+                const double jf = ceil((c - ud) * dN);
+                int j = jf < 0 ? 0 : (jf > dN ? static_cast<int>(N32) : static_cast<int>(jf));
+                while (j > 0 && fma(__int2double_rn(j - 1), delta, ud) >= c) --j;
+                while (j < static_cast<int>(N32) && fma(__int2double_rn(j), delta, ud) < c) ++j;
+                jp = j;
             }
-            shj[threadIdx.x + 1] = jp;
+            shj[threadIdx.x + 1] = static_cast<uint32_t>(jp);
             if (threadIdx.x == 0) shj[0] = jprev;
             __syncthreads();
-            const uint32_t rep = p < N ? shj[threadIdx.x + 1] - shj[threadIdx.x] : 0u;
+            const uint32_t jm = shj[threadIdx.x];
+            const uint32_t rep = p < N32 ? static_cast<uint32_t>(jp) - jm : 0u;
             jprev = shj[THREADS];
-            const unsigned long long v = p < N ? ((rep == 0 ? 1ull : 0ull) | (static_cast<unsigned long long>(rep > 0 ? rep - 1 : 0) << 32)) : 0ull;
-            unsigned long long tot2;
-            const unsigned long long inc = block_inclusive_sum(v, shu, &tot2);
-            const unsigned long long ex = carry2 + inc - v;
-            carry2 += tot2;
-            if (p < N) {
-                sS[p] = static_cast<uint32_t>(ex >> 32);
-                if (rep == 0) {
-                    ep[ex & 0xffffffffull] = static_cast<uint32_t>(p);
+            const bool empty = p < N32 && rep == 0;
+            const unsigned bal = __ballot_sync(0xffffffffu, empty);
+            if (lane == 0) shw[warp] = __popc(bal);
+            __syncthreads();
+            uint32_t before = 0, wtot = 0;
+#pragma unroll
+            for (int w2 = 0; w2 < NW; ++w2) {
+                const uint32_t cw = shw[w2];
+                before += w2 < warp ? cw : 0u;
+                wtot += cw;
+            }
+            const uint32_t E = ecarry + before + __popc(bal & ((1u << lane) - 1u));
+            ecarry += wtot;
+            if (p < N32) {
+                sS[p] = jm + E - p;
+                if (empty) {
+                    ep[E] = p;
                 } else {
                     xn[p] = xc[p];  // occupied slots keep their particle
                     if constexpr (SHADOW) xsn[p] = xsc[p];
@@ -474,20 +496,30 @@ struct FilterRun {
             }
         }
         __syncthreads();
-        n_empty = carry2 & 0xffffffffull;
-        for (uint64_t k = threadIdx.x; k < n_empty; k += THREADS) {
-            uint64_t lo = 0, hi = N;  // last source with surplus prefix <= k
-            while (hi - lo > 1) {
-                const uint64_t mid = (lo + hi) >> 1;
-                if (sS[mid] <= k) {
-                    lo = mid;
-                } else {
-                    hi = mid;
+        n_empty = ecarry;
+        // empty slot k takes the last parent with sS <= k: every thread owns a
+        // run of consecutive empties, finds the first parent by bisection and
+        // walks the parents forward from there
+        {
+            const uint32_t ne = ecarry, per = (ne + THREADS - 1) / THREADS;
+            const uint32_t k0 = threadIdx.x * per, k1 = min(k0 + per, ne);
+            if (k0 < k1) {
+                uint32_t lo = 0, hi = N32;
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (sS[mid] <= k0) {
+                        lo = mid;
+                    } else {
+                        hi = mid;
+                    }
+                }
+                for (uint32_t k = k0; k < k1; ++k) {
+                    while (lo + 1 < N32 && sS[lo + 1] <= k) ++lo;
+                    const uint32_t e = ep[k];
+                    xn[e] = xc[lo];
+                    if constexpr (SHADOW) xsn[e] = xsc[lo];
                 }
             }
-            const uint32_t e = ep[k];
-            xn[e] = xc[lo];
-            if constexpr (SHADOW) xsn[e] = xsc[lo];
         }
         __syncthreads();
         // the gathered particles become the current ones, with equal weights
