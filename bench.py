@@ -49,7 +49,8 @@ buffers directly (rng).
 compiled from its headers into oracle/_ref) on all host threads, on a bounded
 sample of the same workload.
 
-`--parts timed` runs only the warm-up and the timed loop (for profilers).
+`--parts timed` runs only the warm-up and the timed loop (for profilers);
+`--shape 512x2` fixes the batched kernel's block shape instead of autotuning.
 """
 from __future__ import annotations
 
@@ -208,7 +209,12 @@ def bench_smc(args, rank, world, dev):
     w = mb.batched_workload(F=args.filters, T=T, seed=1234 + 7919 * rank)
     ps_per_step = float(w["N"].sum()) * T
     b = make_filters(mb, w)
-    trials = b.autotune()
+    if args.shape:
+        th, cps = (int(v) for v in args.shape.split("x"))
+        b.config(th, cps)
+        trials = [(th, cps, 0.0)]
+    else:
+        trials = b.autotune()
     stream = torch.cuda.current_stream()
     for _ in range(args.warmup):
         b.run(graph=True)
@@ -578,6 +584,7 @@ def main():
     ap.add_argument("--filters", type=int, default=4096)
     ap.add_argument("--obs", type=int, default=500)
     ap.add_argument("--parts", default="all", choices=["all", "timed"])
+    ap.add_argument("--shape", default="", help="threads x CTAs per SM (e.g. 512x2) instead of the autotuner")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -219,13 +219,13 @@ struct ScalarNormal {
 };
 
 // GammaDistribution::generate_{t,w,n,e} (:350-459), the scalar fallback.
-template <typename R, class SW>
+template <typename R, int ALG, class SW>
 __device__ R gamma_scalar(const GammaParam<R> &k, SW &sw, uint64_t &pos)
 {
     using O = GOps<R>;
     const R d = k.d, c = k.c;
     R r = 0;
-    switch (k.alg) {
+    switch (ALG) {
         case 0:
             for (;;) {
                 R u = O::sub(static_cast<R>(1), RealOps<R>::u01(kOO, sw.at(pos++)));
@@ -301,7 +301,7 @@ struct GammaSmem {
 
 // One chunk of n <= K values at stream word `pos`; accepted values go to
 // out[0, m).  Returns m; advances `pos` and `eng` past the chunk's words.
-template <class G, typename W, typename R, int THREADS>
+template <class G, typename W, typename R, int THREADS, int ALG>
 __device__ uint32_t gamma_chunk(const G &g, const GammaParam<R> &k, const Ctr &B, uint32_t off, uint64_t &pos,
     DevEngine<G::kCtrWords> &eng, uint32_t n, R *out, unsigned char *smem, uint32_t *shr, uint64_t *sh_pos)
 {
@@ -311,7 +311,7 @@ __device__ uint32_t gamma_chunk(const G &g, const GammaParam<R> &k, const Ctr &B
     constexpr uint32_t M = static_cast<uint32_t>(WPB);
     const R d = k.d, c = k.c, beta = k.beta;
     // ---- stage this chunk's words
-    const uint64_t nw = (k.alg <= 1) ? 2ull * n : (k.alg == 2 ? 2ull * n + ((n & 1u) ? 2 : 0) : n);
+    const uint64_t nw = (ALG <= 1) ? 2ull * n : (ALG == 2 ? 2ull * n + ((n & 1u) ? 2 : 0) : n);
     uint32_t *st32 = reinterpret_cast<uint32_t *>(smem);
     const W *st = reinterpret_cast<const W *>(st32);
     const uint64_t a0 = static_cast<uint64_t>(off) + pos, b0 = a0 / WPB;
@@ -327,7 +327,7 @@ __device__ uint32_t gamma_chunk(const G &g, const GammaParam<R> &k, const Ctr &B
     R x[EPT];
     bool acc[EPT];
     uint32_t got = 0;
-    if (k.alg == 3) {
+    if constexpr (ALG == 3) {
 #pragma unroll
         for (int j = 0; j < EPT; ++j) {
             const uint32_t i = threadIdx.x + j * THREADS;
@@ -335,7 +335,7 @@ __device__ uint32_t gamma_chunk(const G &g, const GammaParam<R> &k, const Ctr &B
         }
         got = n;
         __syncthreads();
-    } else if (k.alg <= 1) {
+    } else if constexpr (ALG <= 1) {
 #pragma unroll
         for (int j = 0; j < EPT; ++j) {
             const uint32_t i = threadIdx.x + j * THREADS;
@@ -343,7 +343,7 @@ __device__ uint32_t gamma_chunk(const G &g, const GammaParam<R> &k, const Ctr &B
             if (i >= n) continue;
             R u = RealOps<R>::u01(kOO, st[s0 + i]);
             R e = RealOps<R>::u01(kOO, st[s0 + n + i]);
-            if (k.alg == 0) {
+            if constexpr (ALG == 0) {
                 e = O::mul(static_cast<R>(-1), O::log(e));
                 if (u > d) {
                     const R t = O::mul(c, O::sub(static_cast<R>(1), u));
@@ -517,11 +517,11 @@ __device__ uint32_t gamma_chunk(const G &g, const GammaParam<R> &k, const Ctr &B
         for (uint64_t q = 0; q < nscalar; ++q) eng.call(1, M);
         pos += nw + nscalar;
     }
-    if (k.alg != 2) {
-        eng.batch(k.alg <= 1 ? 2ull * n : n, K, M);
+    if constexpr (ALG != 2) {
+        eng.batch(ALG <= 1 ? 2ull * n : n, K, M);
         pos += nw;
     }
-    if (k.alg == 3) return got;
+    if constexpr (ALG == 3) return got;
     // ---- compaction of the accepted values, in index order
     uint32_t m = 0;
 #pragma unroll
@@ -534,13 +534,17 @@ __device__ uint32_t gamma_chunk(const G &g, const GammaParam<R> &k, const Ctr &B
     return m;
 }
 
-// gamma_distribution (:277-302) for `nstreams` streams of n values.  Stream s
-// writes r + s * n; its engine starts at (ctr0 with word 1 = s, empty buffer)
-// when `blocks` is set, else at the engine state given (one stream), whose
-// final state goes to *state_out.
-template <class G, typename W, typename R, int THREADS>
+// gamma_distribution (:277-302) for `nstreams` streams of n values, all of
+// them drawn by algorithm ALG (one instantiation per algorithm keeps the code
+// each SM runs small).  Stream list[i] (i when list is null) writes
+// r + s * n; its engine starts at (ctr0 with word 1 = s, empty buffer) when
+// `blocks` is set, else at the engine state given (one stream), whose final
+// state goes to *ctr_out / *idx_out.
+constexpr int kGammaThreads = 256;
+
+template <class G, typename W, typename R, int THREADS, int ALG>
 __global__ void __launch_bounds__(THREADS, 3) k_gamma(G g, Ctr ctr0, uint32_t idx0, int blocks, uint64_t nstreams,
-    uint64_t n, const GammaParam<R> *params, R *r, Ctr *ctr_out, uint32_t *idx_out)
+    const uint32_t *list, uint64_t n, const GammaParam<R> *params, R *r, Ctr *ctr_out, uint32_t *idx_out)
 {
     using S = GammaSmem<G, W, R>;
     constexpr int K = S::K;
@@ -550,7 +554,8 @@ __global__ void __launch_bounds__(THREADS, 3) k_gamma(G g, Ctr ctr0, uint32_t id
     extern __shared__ __align__(16) unsigned char gamma_dyn[];
     g.prepare();
     unsigned char *smem = gamma_dyn + G::kDynSmem;
-    for (uint64_t sidx = blockIdx.x; sidx < nstreams; sidx += gridDim.x) {
+    for (uint64_t i = blockIdx.x; i < nstreams; i += gridDim.x) {
+        const uint64_t sidx = list ? list[i] : i;
         const GammaParam<R> k = params[blocks ? sidx : 0];
         DevEngine<G::kCtrWords> eng;
         eng.ctr = ctr0;
@@ -571,19 +576,19 @@ __global__ void __launch_bounds__(THREADS, 3) k_gamma(G g, Ctr ctr0, uint32_t id
         uint64_t pos = 0, left = n;
         R *o = r + sidx * n;
         while (left > static_cast<uint64_t>(K)) {
-            const uint32_t m = gamma_chunk<G, W, R, THREADS>(g, k, B, off, pos, eng, K, o, smem, shr, &sh_pos);
+            const uint32_t m = gamma_chunk<G, W, R, THREADS, ALG>(g, k, B, off, pos, eng, K, o, smem, shr, &sh_pos);
             if (m == 0) break;
             left -= m;
             o += m;
         }
-        const uint32_t m = gamma_chunk<G, W, R, THREADS>(g, k, B, off, pos, eng, static_cast<uint32_t>(left), o,
+        const uint32_t m = gamma_chunk<G, W, R, THREADS, ALG>(g, k, B, off, pos, eng, static_cast<uint32_t>(left), o,
             smem, shr, &sh_pos);
         left -= m;
         o += m;
         if (left && threadIdx.x == 0) {
             ScalarWords<G, W> sw{&g, B, off};
             uint64_t sp = pos;
-            for (uint64_t i = 0; i < left; ++i) o[i] = gamma_scalar<R>(k, sw, sp);
+            for (uint64_t q = 0; q < left; ++q) o[q] = gamma_scalar<R, ALG>(k, sw, sp);
             for (uint64_t q = pos; q < sp; ++q) eng.call(1, M);
         }
         if (!blocks && threadIdx.x == 0) {
@@ -594,21 +599,67 @@ __global__ void __launch_bounds__(THREADS, 3) k_gamma(G g, Ctr ctr0, uint32_t id
     }
 }
 
-constexpr int kGammaThreads = 256;
+template <class G, typename W, typename R, int ALG>
+int launch_gamma(const G &g, const Ctr &c0, uint32_t idx0, bool blocks, uint64_t count, const uint32_t *list,
+    uint64_t n, const GammaParam<R> *dparams, R *r, Ctr *dctr, uint32_t *didx, cudaStream_t s)
+{
+    using S = GammaSmem<G, W, R>;
+    auto kern = k_gamma<G, W, R, kGammaThreads, ALG>;
+    const int dyn = G::kDynSmem + S::kBytes;
+    MB_CUDA(allow_dyn_smem(kern, dyn));
+    int per_sm = 0;
+    MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kGammaThreads, dyn));
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint64_t cap = static_cast<uint64_t>(std::max(1, per_sm)) * sms;
+    const unsigned grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(count, cap)));
+    kern<<<grid, kGammaThreads, dyn, s>>>(g, c0, idx0, blocks ? 1 : 0, count, list, n, dparams, r, dctr, didx);
+    MB_LAUNCH_CHECK();
+    return MCKL_B200_OK;
+}
 
+template <class G, typename W, typename R>
+int launch_gamma_alg(int alg, const G &g, const Ctr &c0, uint32_t idx0, bool blocks, uint64_t count,
+    const uint32_t *list, uint64_t n, const GammaParam<R> *dparams, R *r, Ctr *dctr, uint32_t *didx, cudaStream_t s)
+{
+    switch (alg) {
+        case 0: return launch_gamma<G, W, R, 0>(g, c0, idx0, blocks, count, list, n, dparams, r, dctr, didx, s);
+        case 1: return launch_gamma<G, W, R, 1>(g, c0, idx0, blocks, count, list, n, dparams, r, dctr, didx, s);
+        case 2: return launch_gamma<G, W, R, 2>(g, c0, idx0, blocks, count, list, n, dparams, r, dctr, didx, s);
+        default: return launch_gamma<G, W, R, 3>(g, c0, idx0, blocks, count, list, n, dparams, r, dctr, didx, s);
+    }
+}
+
+// One launch per algorithm present: the streams of each algorithm are listed
+// (device copy) so every CTA runs one algorithm's code.
 template <typename R>
 int gamma_impl(mckl_b200_engine_t *e, bool blocks, size_t nstreams, size_t n, const GammaParam<R> *hparams,
     size_t nparams, R *r, void *stream)
 {
     cudaStream_t s = as_stream(stream);
-    // device copies: per-stream constants, final engine state
+    std::vector<uint32_t> lists[4];
+    if (blocks) {
+        for (size_t i = 0; i < nstreams; ++i) lists[hparams[i].alg].push_back(static_cast<uint32_t>(i));
+    }
     const size_t pbytes = align256(nparams * sizeof(GammaParam<R>));
-    char *scr = static_cast<char *>(scratch(6, pbytes + 256, s));
+    const size_t lbytes = align256(blocks ? nstreams * 4 : 4);
+    char *scr = static_cast<char *>(scratch(6, pbytes + lbytes + 256, s));
     if (!scr) return MCKL_B200_ERR_NOMEM;
     auto *dparams = reinterpret_cast<GammaParam<R> *>(scr);
-    Ctr *dctr = reinterpret_cast<Ctr *>(scr + pbytes);
-    uint32_t *didx = reinterpret_cast<uint32_t *>(scr + pbytes + sizeof(Ctr));
+    uint32_t *dlist = reinterpret_cast<uint32_t *>(scr + pbytes);
+    Ctr *dctr = reinterpret_cast<Ctr *>(scr + pbytes + lbytes);
+    uint32_t *didx = reinterpret_cast<uint32_t *>(scr + pbytes + lbytes + sizeof(Ctr));
     MB_CUDA(cudaMemcpyAsync(dparams, hparams, nparams * sizeof(GammaParam<R>), cudaMemcpyHostToDevice, s));
+    std::vector<uint32_t> flat;
+    size_t first[4] = {0, 0, 0, 0};
+    if (blocks) {
+        for (int a = 0; a < 4; ++a) {
+            first[a] = flat.size();
+            flat.insert(flat.end(), lists[a].begin(), lists[a].end());
+        }
+        MB_CUDA(cudaMemcpyAsync(dlist, flat.data(), flat.size() * 4, cudaMemcpyHostToDevice, s));
+    }
     const Ctr c0 = ctr_of(*e);
     const uint32_t idx0 = e->index;
     const bool w64 = geom(e->kind).rbytes == 8;
@@ -616,19 +667,16 @@ int gamma_impl(mckl_b200_engine_t *e, bool blocks, size_t nstreams, size_t n, co
         using G = decltype(g);
         auto run = [&](auto wtag) {
             using W = decltype(wtag);
-            using S = GammaSmem<G, W, R>;
-            auto kern = k_gamma<G, W, R, kGammaThreads>;
-            const int dyn = G::kDynSmem + S::kBytes;
-            MB_CUDA(allow_dyn_smem(kern, dyn));
-            int per_sm = 0;
-            MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kGammaThreads, dyn));
-            int dev = 0, sms = 148;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            const uint64_t cap = static_cast<uint64_t>(std::max(1, per_sm)) * sms;
-            const unsigned grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(nstreams, cap)));
-            kern<<<grid, kGammaThreads, dyn, s>>>(g, c0, idx0, blocks ? 1 : 0, nstreams, n, dparams, r, dctr, didx);
-            MB_LAUNCH_CHECK();
+            if (!blocks) {
+                return launch_gamma_alg<G, W, R>(hparams[0].alg, g, c0, idx0, false, 1, nullptr, n, dparams, r, dctr,
+                    didx, s);
+            }
+            for (int a = 0; a < 4; ++a) {
+                if (lists[a].empty()) continue;
+                const int rc2 = launch_gamma_alg<G, W, R>(a, g, c0, idx0, true, lists[a].size(), dlist + first[a], n,
+                    dparams, r, dctr, didx, s);
+                if (rc2 != MCKL_B200_OK) return rc2;
+            }
             return MCKL_B200_OK;
         };
         if (w64) return run(uint64_t{});
@@ -643,6 +691,9 @@ int gamma_impl(mckl_b200_engine_t *e, bool blocks, size_t nstreams, size_t n, co
         MB_CUDA(cudaStreamSynchronize(s));
         set_ctr(*e, hc);
         e->index = hi;
+    } else {
+        // the host lists must outlive the asynchronous copies
+        MB_CUDA(cudaStreamSynchronize(s));
     }
     return MCKL_B200_OK;
 }
