@@ -217,6 +217,9 @@ struct Step {
 // angle words of the block 128 further on, i.e. up to four pairs for two
 // Philox blocks (a quarter block per particle).  Units past the full chunks
 // are the pairs of the last partial chunk, drawn word by word.
+// Parents with many copies that the CTA copies together (per resampling).
+constexpr uint32_t kBigParents = 64;
+
 struct NoiseLayout {
     static constexpr uint64_t kUnits = 129;  // units per full chunk
     uint64_t N, m, tail, nu_tail, units, per_step;
@@ -435,89 +438,132 @@ struct FilterRun {
         }
         const double U = __dadd_rn(__dmul_rn(static_cast<double>(wr[0]), 0x1p-64),
             __dmul_rn(static_cast<double>(wr[1]), 0x1p-32));
-        const double delta = 1.0 / static_cast<double>(N);
-        const double ud = U * delta;
         const double invS = 1.0 / S;
-        // per tile of THREADS particles: inclusive FP64 scan of the
-        // normalised weights; cumulative counts j_p = #{k : u_k < c_p} (the
-        // lower bound of c_p on the grid fma(k, delta, ud)); replication
-        // counts rep_p = j_p - j_{p-1}; the empty slots (rep = 0) in order,
-        // ranked by a CTA ballot; and the surplus copies of the parents
-        // before p, sS_p = sum_{i<p} max(rep_i - 1, 0) = j_{p-1} - p + E_p
-        // with E_p the empty slots before p
-        constexpr int NW = THREADS / 32;
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        uint32_t *shw = reinterpret_cast<uint32_t *>(shu);
+        // Exact fixed-point systematic resampling.  The normalised weights
+        // become integers W_p = RN(w_p 2^62) (absolute error 2^-63 each) and
+        // are summed exactly in 64 bits: the cumulative weights C_p are exact,
+        // monotone and independent of the summation order.  The count of grid
+        // points (U + j) / N below C_p 2^-62 is then exact integer arithmetic:
+        // j_p = clamp(ceil((4 N C_p - U 2^64) / 2^64), 0, N), with U the
+        // canonical double of the two resampling words (a multiple of 2^-64).
+        // Each thread owns V consecutive particles per tile of THREADS x V.
+        // From the counts: replication counts rep_p = j_p - j_{p-1}, the
+        // empty slots (rep = 0) in order, and the surplus copies of the
+        // parents before p, sS_p = sum_{i<p} max(rep_i - 1, 0) = j_{p-1} - p
+        // + E_p with E_p the empty slots before p.
+        constexpr int V = 8;
+        constexpr uint32_t TILE = THREADS * V;
+        const uint64_t U64 = U < 1.0 ? static_cast<uint64_t>(U * 0x1p64) : ~0ull;
         const uint32_t N32 = static_cast<uint32_t>(N);
-        const double dN = static_cast<double>(N);
-        double carry = 0.0;
+        unsigned long long *shw64 = shu;
+        uint64_t carry = 0;
         uint32_t jprev = 0, ecarry = 0;
-        for (uint32_t b = 0; b < N32; b += THREADS) {
-            const uint32_t p = b + threadIdx.x;
-            const double w = p < N32 ? static_cast<double>(Math<R>::exp(Math<R>::sub(st.l[p], M))) * invS : 0.0;
-            double tot;
-            const double c = carry + block_inclusive_sum(w, shd, &tot);
-            carry += tot;
-            int jp = static_cast<int>(N32);
-            if (p + 1 < N32) {
-                const double jf = ceil((c - ud) * dN);
-                int j = jf < 0 ? 0 : (jf > dN ? static_cast<int>(N32) : static_cast<int>(jf));
-                while (j > 0 && fma(__int2double_rn(j - 1), delta, ud) >= c) --j;
-                while (j < static_cast<int>(N32) && fma(__int2double_rn(j), delta, ud) < c) ++j;
-                jp = j;
+        for (uint32_t b = 0; b < N32; b += TILE) {
+            const uint32_t q0 = b + threadIdx.x * V;
+            unsigned long long C[V];
+            unsigned long long acc = 0;
+#pragma unroll
+            for (int k = 0; k < V; ++k) {
+                const uint32_t p = q0 + k;
+                const double w = p < N32 ? static_cast<double>(Math<R>::exp(Math<R>::sub(st.l[p], M))) * invS : 0.0;
+                acc += __double2ull_rn(w * 0x1p62);
+                C[k] = acc;
             }
-            shj[threadIdx.x + 1] = static_cast<uint32_t>(jp);
+            unsigned long long tot;
+            const uint64_t excl = block_inclusive_sum(acc, shw64, &tot) - acc;
+            const uint64_t base = carry + excl;
+            carry += tot;
+            uint32_t j[V];
+#pragma unroll
+            for (int k = 0; k < V; ++k) {
+                const uint32_t p = q0 + k;
+                const uint64_t c = base + C[k];
+                // X = 4 N c as a 128-bit number (hi, lo)
+                const uint64_t lo = static_cast<uint64_t>(N32) * c, hi = __umul64hi(static_cast<uint64_t>(N32), c);
+                const uint64_t xhi = (hi << 2) | (lo >> 62), xlo = lo << 2;
+                uint32_t cnt;
+                if (xhi == 0 && xlo <= U64) {
+                    cnt = 0;
+                } else {
+                    // floor((X - U64 - 1) / 2^64) + 1: the high word of
+                    // X - (U64 + 1), plus one
+                    const uint64_t borrow = (U64 == ~0ull || xlo < U64 + 1) ? 1 : 0;
+                    const uint64_t dhi = xhi - borrow;
+                    cnt = dhi + 1 > N32 ? N32 : static_cast<uint32_t>(dhi + 1);
+                }
+                j[k] = (p + 1 >= N32) ? N32 : cnt;
+            }
+            shj[threadIdx.x + 1] = j[V - 1];
             if (threadIdx.x == 0) shj[0] = jprev;
             __syncthreads();
-            const uint32_t jm = shj[threadIdx.x];
-            const uint32_t rep = p < N32 ? static_cast<uint32_t>(jp) - jm : 0u;
+            uint32_t jm = shj[threadIdx.x];
             jprev = shj[THREADS];
-            const bool empty = p < N32 && rep == 0;
-            const unsigned bal = __ballot_sync(0xffffffffu, empty);
-            if (lane == 0) shw[warp] = __popc(bal);
-            __syncthreads();
-            uint32_t before = 0, wtot = 0;
+            uint32_t ne = 0;
 #pragma unroll
-            for (int w2 = 0; w2 < NW; ++w2) {
-                const uint32_t cw = shw[w2];
-                before += w2 < warp ? cw : 0u;
-                wtot += cw;
+            for (int k = 0; k < V; ++k) {
+                const uint32_t p = q0 + k;
+                const uint32_t jk = j[k];
+                ne += (p < N32 && jk == (k == 0 ? jm : j[k - 1])) ? 1u : 0u;
             }
-            const uint32_t E = ecarry + before + __popc(bal & ((1u << lane) - 1u));
-            ecarry += wtot;
-            if (p < N32) {
-                sS[p] = jm + E - p;
-                if (empty) {
-                    ep[E] = p;
-                } else {
-                    xn[p] = xc[p];  // occupied slots keep their particle
-                    if constexpr (SHADOW) xsn[p] = xsc[p];
+            uint32_t etot;
+            const uint32_t eex = block_inclusive_sum(ne, shj + THREADS + 1, &etot) - ne;
+            uint32_t E = ecarry + eex;
+            ecarry += etot;
+#pragma unroll
+            for (int k = 0; k < V; ++k) {
+                const uint32_t p = q0 + k;
+                if (p < N32) {
+                    const uint32_t jb = k == 0 ? jm : j[k - 1];
+                    sS[p] = jb + E - p;
+                    if (j[k] == jb) {
+                        ep[E] = p;
+                        ++E;
+                    } else {
+                        xn[p] = xc[p];  // occupied slots keep their particle
+                        if constexpr (SHADOW) xsn[p] = xsc[p];
+                    }
                 }
             }
         }
         __syncthreads();
         n_empty = ecarry;
-        // empty slot k takes the last parent with sS <= k: every thread owns a
-        // run of consecutive empties, finds the first parent by bisection and
-        // walks the parents forward from there
+        // parent p fills the empty slots ep[sS_p, sS_{p+1}) with copies of
+        // itself (empty slot k takes the last parent with sS <= k); parents
+        // with more than 32 copies are queued and copied by the whole CTA
         {
-            const uint32_t ne = ecarry, per = (ne + THREADS - 1) / THREADS;
-            const uint32_t k0 = threadIdx.x * per, k1 = min(k0 + per, ne);
-            if (k0 < k1) {
-                uint32_t lo = 0, hi = N32;
-                while (hi - lo > 1) {
-                    const uint32_t mid = (lo + hi) >> 1;
-                    if (sS[mid] <= k0) {
-                        lo = mid;
-                    } else {
-                        hi = mid;
+            uint32_t *nbig = shj + THREADS + 34;  // queue length, then queued parents
+            uint32_t *big = nbig + 1;
+            if (threadIdx.x == 0) *nbig = 0;
+            __syncthreads();
+            const uint32_t ne = ecarry;
+            for (uint32_t p = threadIdx.x; p < N32; p += THREADS) {
+                const uint32_t s0 = sS[p], s1 = p + 1 < N32 ? sS[p + 1] : ne;
+                if (s1 - s0 > 32) {
+                    const uint32_t q = atomicAdd(nbig, 1u);
+                    if (q < kBigParents) {
+                        big[q] = p;
+                        continue;
                     }
                 }
-                for (uint32_t k = k0; k < k1; ++k) {
-                    while (lo + 1 < N32 && sS[lo + 1] <= k) ++lo;
+                const R v = xc[p];
+                double vs = 0.0;
+                if constexpr (SHADOW) vs = xsc[p];
+                for (uint32_t k = s0; k < s1; ++k) {
                     const uint32_t e = ep[k];
-                    xn[e] = xc[lo];
-                    if constexpr (SHADOW) xsn[e] = xsc[lo];
+                    xn[e] = v;
+                    if constexpr (SHADOW) xsn[e] = vs;
+                }
+            }
+            __syncthreads();
+            const uint32_t nb = min(*nbig, kBigParents);
+            for (uint32_t i = 0; i < nb; ++i) {
+                const uint32_t p = big[i];
+                const uint32_t s0 = sS[p], s1 = p + 1 < N32 ? sS[p + 1] : ne;
+                const R v = xc[p];
+                for (uint32_t k = s0 + threadIdx.x; k < s1; k += THREADS) {
+                    const uint32_t e = ep[k];
+                    xn[e] = v;
+                    if constexpr (SHADOW) xsn[e] = xsc[p];
                 }
             }
         }
@@ -547,7 +593,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_pf_batched(const BatchedFilte
     __shared__ double shd[33];
     __shared__ R shr[33];
     __shared__ unsigned long long shu[33];
-    __shared__ uint32_t shj[THREADS + 1];
+    __shared__ uint32_t shj[THREADS + 35 + kBigParents];
     __shared__ int sh_f;
     while (true) {
         if (threadIdx.x == 0) {
@@ -617,7 +663,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_adjoint(const BatchedFilter *
 {
     __shared__ double shd[33];
     __shared__ unsigned long long shu[33];
-    __shared__ uint32_t shj[THREADS + 1];
+    __shared__ uint32_t shj[THREADS + 35 + kBigParents];
     __shared__ int sh_f;
     const int C = A.C;
     const uint64_t slot = blockIdx.x, cn = static_cast<uint64_t>(C) * A.nmax;
