@@ -303,8 +303,9 @@ struct FilterRun {
     NoiseLayout lay;
     PhiloxGen gm, gr;
     Step<R, SHADOW> st;
-    R *xc, *xn;
-    double *xsc, *xsn;
+    R *xc;
+    double *xsc;
+    double *rec_x = nullptr;  // when set: each step's particles before resampling
     uint32_t *sS, *ep;
     double threshold;
     double L_prev, ll_sum, Ls_prev, lls_sum;
@@ -316,10 +317,10 @@ struct FilterRun {
         lay.init(F.n);
         gm = PhiloxGen{F.mkey[0], F.mkey[1]};
         gr = PhiloxGen{F.rkey[0], F.rkey[1]};
+        (void) xb;
+        (void) xsb;
         xc = xa + F.off;
-        xn = xb + F.off;
         xsc = SHADOW ? xsa + F.off : nullptr;
-        xsn = SHADOW ? xsb + F.off : nullptr;
         sS = scanS + F.off;
         ep = epos + F.off;
         threshold = thr;
@@ -364,8 +365,9 @@ struct FilterRun {
     }
 
     // Step t: move, weight, normalise and (when ESS < N threshold) resample;
-    // returns whether it resampled.  After a resampling the particles before
-    // it are still in xn, the placement in sS / ep[0, n_empty).
+    // returns whether it resampled.  The resampling is in place (an empty
+    // slot takes a copy of an occupied one, which is never overwritten); its
+    // placement stays in sS / ep[0, n_empty).
     __device__ bool step(int t, double yt_d, double *shd, R *shr, unsigned long long *shu, uint32_t *shj)
     {
         const uint64_t N = lay.N;
@@ -425,6 +427,10 @@ struct FilterRun {
         }
         st.lshift = M;
         st.flat = false;
+        if (rec_x) {
+            for (uint64_t p = threadIdx.x; p < N; p += THREADS) rec_x[p] = static_cast<double>(xc[p]);
+            __syncthreads();  // the resampling below overwrites empty slots in place
+        }
         const double ess = S * S / Q;
         if (!(ess < static_cast<double>(N) * threshold)) return false;
         // ---- systematic resampling
@@ -518,9 +524,6 @@ struct FilterRun {
                     if (j[k] == jb) {
                         ep[E] = p;
                         ++E;
-                    } else {
-                        xn[p] = xc[p];  // occupied slots keep their particle
-                        if constexpr (SHADOW) xsn[p] = xsc[p];
                     }
                 }
             }
@@ -550,8 +553,8 @@ struct FilterRun {
                 if constexpr (SHADOW) vs = xsc[p];
                 for (uint32_t k = s0; k < s1; ++k) {
                     const uint32_t e = ep[k];
-                    xn[e] = v;
-                    if constexpr (SHADOW) xsn[e] = vs;
+                    xc[e] = v;
+                    if constexpr (SHADOW) xsc[e] = vs;
                 }
             }
             __syncthreads();
@@ -562,21 +565,13 @@ struct FilterRun {
                 const R v = xc[p];
                 for (uint32_t k = s0 + threadIdx.x; k < s1; k += THREADS) {
                     const uint32_t e = ep[k];
-                    xn[e] = v;
-                    if constexpr (SHADOW) xsn[e] = xsc[p];
+                    xc[e] = v;
+                    if constexpr (SHADOW) xsc[e] = xsc[p];
                 }
             }
         }
         __syncthreads();
-        // the gathered particles become the current ones, with equal weights
-        R *tx = xc;
-        xc = xn;
-        xn = tx;
-        if constexpr (SHADOW) {
-            double *ts = xsc;
-            xsc = xsn;
-            xsn = ts;
-        }
+        // the particles now carry equal weights
         st.flat = true;
         L_prev = log(static_cast<double>(N));
         Ls_prev = L_prev;
@@ -752,14 +747,14 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_adjoint(const BatchedFilter *
             }
             for (int t = t0 + 1; t <= t1; ++t) {
                 const uint64_t q = static_cast<uint64_t>(t - t0 - 1);
-                const bool res = run.step(t, yf[t], shd, shd, shu, shj);
-                // record: particles before any resampling, log-weights, and
-                // the parent placement (occupied flags, surplus prefix, empties)
-                const double *xpre = res ? run.xn : run.xc;
                 double *qx = rx + q * A.nmax, *ql = rl + q * A.nmax;
+                run.rec_x = qx;  // the step records its particles before resampling
+                const bool res = run.step(t, yf[t], shd, shd, shu, shj);
+                run.rec_x = nullptr;
+                // record the log-weights and the parent placement (occupied
+                // flags, surplus prefix, empties)
                 uint32_t *qo = rrep + q * A.nmax, *qs = rsS + q * A.nmax, *qe = rep_list + q * A.nmax;
                 for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
-                    qx[p] = xpre[p];
                     ql[p] = run.st.l[p];
                     if (res) {
                         qo[p] = 1;
@@ -1043,9 +1038,9 @@ int mckl_b200_batched_create(mckl_b200_batched_t **out, size_t F, const size_t *
     const bool shadow = (fp64 >= 2);
     b->fp64 = (fp64 == 1 || fp64 == 3) ? 1 : 0;
     const size_t rs = b->fp64 ? 8 : 4;
-    const size_t bytes = align256(F * sizeof(BatchedFilter)) + align256(F * (T + 1) * 8) + 3 * align256(total * rs) +
+    const size_t bytes = align256(F * sizeof(BatchedFilter)) + align256(F * (T + 1) * 8) + 2 * align256(total * rs) +
                          2 * align256(total * 4) + align256(F * 8) + align256(F * 4) + align256(F * 4) + 256 +
-                         (shadow ? 3 * align256(total * 8) + align256(F * 8) : 0);
+                         (shadow ? 2 * align256(total * 8) + align256(F * 8) : 0);
     if (cudaMalloc(&b->mem, bytes) != cudaSuccess) {
         delete b;
         set_error("batched filter allocation failed");
@@ -1060,7 +1055,7 @@ int mckl_b200_batched_create(mckl_b200_batched_t **out, size_t F, const size_t *
     b->a.filt = reinterpret_cast<BatchedFilter *>(take(F * sizeof(BatchedFilter)));
     b->a.y = reinterpret_cast<double *>(take(F * (T + 1) * 8));
     b->a.xa = take(total * rs);
-    b->a.xb = take(total * rs);
+    b->a.xb = nullptr;  // the resampling gathers in place
     b->a.lw = take(total * rs);
     b->a.scanS = reinterpret_cast<uint32_t *>(take(total * 4));
     b->a.epos = reinterpret_cast<uint32_t *>(take(total * 4));
@@ -1070,7 +1065,7 @@ int mckl_b200_batched_create(mckl_b200_batched_t **out, size_t F, const size_t *
     b->queue = reinterpret_cast<int *>(take(256));
     if (shadow) {
         b->a.xsa = reinterpret_cast<double *>(take(total * 8));
-        b->a.xsb = reinterpret_cast<double *>(take(total * 8));
+        b->a.xsb = nullptr;
         b->a.lws = reinterpret_cast<double *>(take(total * 8));
         b->a.loglik_shadow = reinterpret_cast<double *>(take(F * 8));
     }

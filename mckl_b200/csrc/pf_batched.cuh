@@ -23,7 +23,7 @@ struct BatchedArgs {
     int T;
     double threshold;
     int fp64;           // 1: propagate in double, 0: in float
-    void *xa, *xb, *lw; // particles (two buffers, swapped at each resampling), log-weights
+    void *xa, *xb, *lw; // particles (resampled in place; xb unused), log-weights
     uint32_t *scanS, *epos;
     double *loglik;
     uint32_t *nresampled;
