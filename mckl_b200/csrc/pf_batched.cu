@@ -163,50 +163,100 @@ struct Step {
     double phi_d, sx_d, sd0_d, lconst_d, hinv_d, yt_d, lshift_s;
     bool init, flat;
 
-    __device__ __forceinline__ void pair(uint32_t wrad, uint32_t wang, uint64_t p0, uint64_t p1, R *v, double *vs) const
+    // the move and weight of one particle from its old state (registers)
+    __device__ __forceinline__ R move(R e, R x_old, R l_old, R &v) const
     {
-        const R rr = Math<R>::radius(u01oc<R>(wrad));
-        R sn, cs;
-        Math<R>::sincos2pi(u01oc<R>(wang), &sn, &cs);
-        one(Math<R>::mul(rr, sn), p0, v[0]);
-        one(Math<R>::mul(rr, cs), p1, v[1]);
-        if constexpr (SHADOW) {
-            const double rd = Math<double>::radius(u01oc<double>(wrad));
-            double snd, csd;
-            Math<double>::sincos2pi(u01oc<double>(wang), &snd, &csd);
-            one_shadow(__dmul_rn(rd, snd), p0, vs[0]);
-            one_shadow(__dmul_rn(rd, csd), p1, vs[1]);
-        }
+        using O = Math<R>;
+        if (init) return O::mul(sd0, e);
+        const R xn = O::fma(phi, x_old, O::mul(sx, e));
+        const R r = O::sub(yt, xn);
+        const R lo = flat ? R(0) : O::sub(l_old, lshift);
+        v = O::add(lo, O::fma(-O::mul(r, r), hinv, lconst));
+        return xn;
+    }
+
+    __device__ __forceinline__ double move_shadow(double e, double x_old, double l_old, double &v) const
+    {
+        using O = Math<double>;
+        if (init) return O::mul(sd0_d, e);
+        const double xn = O::fma(phi_d, x_old, O::mul(sx_d, e));
+        const double r = O::sub(yt_d, xn);
+        const double lo = flat ? 0.0 : O::sub(l_old, lshift_s);
+        v = O::add(lo, O::fma(-O::mul(r, r), hinv_d, lconst_d));
+        return xn;
     }
 
     __device__ __forceinline__ void one(R e, uint64_t p, R &v) const
     {
-        using O = Math<R>;
-        if (init) {
-            x[p] = O::mul(sd0, e);
-            return;
-        }
-        const R xn = O::fma(phi, x[p], O::mul(sx, e));
+        const R xn = move(e, init ? R(0) : x[p], (init || flat) ? R(0) : l[p], v);
         x[p] = xn;
-        const R r = O::sub(yt, xn);
-        const R lo = flat ? R(0) : O::sub(l[p], lshift);
-        v = O::add(lo, O::fma(-O::mul(r, r), hinv, lconst));
-        l[p] = v;
+        if (!init) l[p] = v;
     }
 
     __device__ __forceinline__ void one_shadow(double e, uint64_t p, double &v) const
     {
-        using O = Math<double>;
-        if (init) {
-            xs[p] = O::mul(sd0_d, e);
-            return;
-        }
-        const double xn = O::fma(phi_d, xs[p], O::mul(sx_d, e));
+        const double xn = move_shadow(e, init ? 0.0 : xs[p], (init || flat) ? 0.0 : ls[p], v);
         xs[p] = xn;
-        const double r = O::sub(yt_d, xn);
-        const double lo = flat ? 0.0 : O::sub(ls[p], lshift_s);
-        v = O::add(lo, O::fma(-O::mul(r, r), hinv_d, lconst_d));
-        ls[p] = v;
+        if (!init) ls[p] = v;
+    }
+
+    // Four pairs of one unit: every load of the unit is issued before any
+    // store, so the loads overlap instead of queueing behind the stores.
+    __device__ __forceinline__ void unit4(const uint32_t (&wr)[4], const uint32_t (&wa)[4],
+        const uint32_t (&pa)[4], const uint32_t (&pb)[4], int lo, int hi, R *v, double *vs) const
+    {
+        R xo[8], lo_[8];
+        double xso[8], lso[8];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            xo[2 * j] = xo[2 * j + 1] = lo_[2 * j] = lo_[2 * j + 1] = R(0);
+            xso[2 * j] = xso[2 * j + 1] = lso[2 * j] = lso[2 * j + 1] = 0.0;
+            if (j >= lo && j < hi && !init) {
+                xo[2 * j] = x[pa[j]];
+                xo[2 * j + 1] = x[pb[j]];
+                if (!flat) {
+                    lo_[2 * j] = l[pa[j]];
+                    lo_[2 * j + 1] = l[pb[j]];
+                }
+                if constexpr (SHADOW) {
+                    xso[2 * j] = xs[pa[j]];
+                    xso[2 * j + 1] = xs[pb[j]];
+                    if (!flat) {
+                        lso[2 * j] = ls[pa[j]];
+                        lso[2 * j + 1] = ls[pb[j]];
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (j >= lo && j < hi) {
+                const R rr = Math<R>::radius(u01oc<R>(wr[j]));
+                R sn, cs;
+                Math<R>::sincos2pi(u01oc<R>(wa[j]), &sn, &cs);
+                const R x0 = move(Math<R>::mul(rr, sn), xo[2 * j], lo_[2 * j], v[2 * j]);
+                const R x1 = move(Math<R>::mul(rr, cs), xo[2 * j + 1], lo_[2 * j + 1], v[2 * j + 1]);
+                x[pa[j]] = x0;
+                x[pb[j]] = x1;
+                if (!init) {
+                    l[pa[j]] = v[2 * j];
+                    l[pb[j]] = v[2 * j + 1];
+                }
+                if constexpr (SHADOW) {
+                    const double rd = Math<double>::radius(u01oc<double>(wr[j]));
+                    double snd, csd;
+                    Math<double>::sincos2pi(u01oc<double>(wa[j]), &snd, &csd);
+                    const double s0 = move_shadow(__dmul_rn(rd, snd), xso[2 * j], lso[2 * j], vs[2 * j]);
+                    const double s1 = move_shadow(__dmul_rn(rd, csd), xso[2 * j + 1], lso[2 * j + 1], vs[2 * j + 1]);
+                    xs[pa[j]] = s0;
+                    xs[pb[j]] = s1;
+                    if (!init) {
+                        ls[pa[j]] = vs[2 * j];
+                        ls[pb[j]] = vs[2 * j + 1];
+                    }
+                }
+            }
+        }
     }
 };
 
@@ -266,6 +316,39 @@ struct NoiseLayout {
             const uint32_t wrad = word_at(gm, base + i, wc);
             const uint32_t wang = word_at(gm, base + nu_tail + i, wc);
             pair(wrad, wang, m * 1024 + i, m * 1024 + nu_tail + i, 0);
+            *lo_out = 0;
+            *hi_out = 1;
+        }
+    }
+
+    // The words and particle indices of unit u at step t: pairs j in
+    // [lo, hi) use words wr[j], wa[j] and move particles pa[j], pb[j].
+    __device__ __forceinline__ void decode(const PhiloxGen &gm, int t, uint64_t u, uint32_t (&wr)[4],
+        uint32_t (&wa)[4], uint32_t (&pa)[4], uint32_t (&pb)[4], int *lo_out, int *hi_out) const
+    {
+        const uint64_t P = static_cast<uint64_t>(t) * per_step;
+        if (u < m * kUnits) {
+            const uint64_t c = u / kUnits, g = u % kUnits;
+            const uint64_t base = P + c * 1024;
+            const uint64_t B = (base >> 2) + g;
+            const int i0 = static_cast<int>(4 * g) - static_cast<int>(base & 3);
+            gm.block(Ctr{{B + 1, 0, 0, 0}}, wr);
+            gm.block(Ctr{{B + 129, 0, 0, 0}}, wa);
+            *lo_out = i0 < 0 ? -i0 : 0;
+            *hi_out = i0 + 4 > 512 ? 512 - i0 : 4;
+            const uint32_t q = static_cast<uint32_t>(c * 1024) + static_cast<uint32_t>(i0);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                pa[j] = q + j;  // only [lo, hi) are used
+                pb[j] = q + j + 512;
+            }
+        } else {
+            const uint64_t i = u - m * kUnits, base = P + m * 1024;
+            WordCache wc{~0ull, {0, 0, 0, 0}};
+            wr[0] = word_at(gm, base + i, wc);
+            wa[0] = word_at(gm, base + nu_tail + i, wc);
+            pa[0] = static_cast<uint32_t>(m * 1024 + i);
+            pb[0] = static_cast<uint32_t>(m * 1024 + nu_tail + i);
             *lo_out = 0;
             *hi_out = 1;
         }
@@ -383,9 +466,9 @@ struct FilterRun {
             R v[8];
             double vs[8];
             int lo, hi;
-            lay.unit(gm, t, u, &lo, &hi, [&](uint32_t wrad, uint32_t wang, uint64_t p0, uint64_t p1, int j) {
-                st.pair(wrad, wang, p0, p1, v + 2 * j, vs + 2 * j);
-            });
+            uint32_t wr[4], wa[4], pa[4], pb[4];
+            lay.decode(gm, t, u, wr, wa, pa, pb, &lo, &hi);
+            st.unit4(wr, wa, pa, pb, lo, hi, v, vs);
             if (t > 0) {
                 acc.add(v, 2 * lo, 2 * hi);
                 if constexpr (SHADOW) accs.add(vs, 2 * lo, 2 * hi);
@@ -539,22 +622,35 @@ struct FilterRun {
             if (threadIdx.x == 0) *nbig = 0;
             __syncthreads();
             const uint32_t ne = ecarry;
-            for (uint32_t p = threadIdx.x; p < N32; p += THREADS) {
-                const uint32_t s0 = sS[p], s1 = p + 1 < N32 ? sS[p + 1] : ne;
-                if (s1 - s0 > 32) {
-                    const uint32_t q = atomicAdd(nbig, 1u);
-                    if (q < kBigParents) {
-                        big[q] = p;
-                        continue;
-                    }
+            // V consecutive parents per thread; their prefixes and particles
+            // are loaded before any copy is stored
+            for (uint32_t q0 = threadIdx.x * V; q0 < N32; q0 += TILE) {
+                uint32_t ss[V + 1];
+                R xv[V];
+                double xsv[V];
+#pragma unroll
+                for (int k = 0; k <= V; ++k) ss[k] = q0 + k < N32 ? sS[q0 + k] : ne;
+#pragma unroll
+                for (int k = 0; k < V; ++k) {
+                    xv[k] = q0 + k < N32 ? xc[q0 + k] : R(0);
+                    if constexpr (SHADOW) xsv[k] = q0 + k < N32 ? xsc[q0 + k] : 0.0;
                 }
-                const R v = xc[p];
-                double vs = 0.0;
-                if constexpr (SHADOW) vs = xsc[p];
-                for (uint32_t k = s0; k < s1; ++k) {
-                    const uint32_t e = ep[k];
-                    xc[e] = v;
-                    if constexpr (SHADOW) xsc[e] = vs;
+#pragma unroll
+                for (int k = 0; k < V; ++k) {
+                    const uint32_t s0 = ss[k], s1 = ss[k + 1];
+                    if (q0 + k >= N32 || s1 <= s0) continue;
+                    if (s1 - s0 > 32) {
+                        const uint32_t q = atomicAdd(nbig, 1u);
+                        if (q < kBigParents) {
+                            big[q] = q0 + k;
+                            continue;
+                        }
+                    }
+                    for (uint32_t c = s0; c < s1; ++c) {
+                        const uint32_t e = ep[c];
+                        xc[e] = xv[k];
+                        if constexpr (SHADOW) xsc[e] = xsv[k];
+                    }
                 }
             }
             __syncthreads();
