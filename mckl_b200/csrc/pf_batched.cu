@@ -270,6 +270,39 @@ struct Step {
 // Parents with many copies that the CTA copies together (per resampling).
 constexpr uint32_t kBigParents = 64;
 
+// Eight consecutive elements starting at a 32-byte aligned address (float,
+// uint32) or a 64-byte aligned one (double) with vector loads and stores.
+// Every filter's particle range starts on a multiple of 32 elements.
+__device__ __forceinline__ void ld8(const float *p, float (&v)[8])
+{
+    const float4 a = reinterpret_cast<const float4 *>(p)[0], b = reinterpret_cast<const float4 *>(p)[1];
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+}
+
+__device__ __forceinline__ void ld8(const double *p, double (&v)[8])
+{
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const double2 a = reinterpret_cast<const double2 *>(p)[q];
+        v[2 * q] = a.x;
+        v[2 * q + 1] = a.y;
+    }
+}
+
+__device__ __forceinline__ void ld8(const uint32_t *p, uint32_t (&v)[8])
+{
+    const uint4 a = reinterpret_cast<const uint4 *>(p)[0], b = reinterpret_cast<const uint4 *>(p)[1];
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+}
+
+__device__ __forceinline__ void st8(uint32_t *p, const uint32_t (&v)[8])
+{
+    reinterpret_cast<uint4 *>(p)[0] = make_uint4(v[0], v[1], v[2], v[3]);
+    reinterpret_cast<uint4 *>(p)[1] = make_uint4(v[4], v[5], v[6], v[7]);
+}
+
 struct NoiseLayout {
     static constexpr uint64_t kUnits = 129;  // units per full chunk
     uint64_t N, m, tail, nu_tail, units, per_step;
@@ -549,12 +582,19 @@ struct FilterRun {
         uint32_t jprev = 0, ecarry = 0;
         for (uint32_t b = 0; b < N32; b += TILE) {
             const uint32_t q0 = b + threadIdx.x * V;
+            const bool whole = q0 + V <= N32;  // all V particles exist
+            R lv[V];
+            if (whole) {
+                ld8(st.l + q0, lv);
+            } else {
+#pragma unroll
+                for (int k = 0; k < V; ++k) lv[k] = q0 + k < N32 ? st.l[q0 + k] : R(0);
+            }
             unsigned long long C[V];
             unsigned long long acc = 0;
 #pragma unroll
             for (int k = 0; k < V; ++k) {
-                const uint32_t p = q0 + k;
-                const double w = p < N32 ? static_cast<double>(Math<R>::exp(Math<R>::sub(st.l[p], M))) * invS : 0.0;
+                const double w = (whole || q0 + k < N32) ? static_cast<double>(Math<R>::exp(Math<R>::sub(lv[k], M))) * invS : 0.0;
                 acc += __double2ull_rn(w * 0x1p62);
                 C[k] = acc;
             }
@@ -598,17 +638,23 @@ struct FilterRun {
             const uint32_t eex = block_inclusive_sum(ne, shj + THREADS + 1, &etot) - ne;
             uint32_t E = ecarry + eex;
             ecarry += etot;
+            uint32_t sv[V];
 #pragma unroll
             for (int k = 0; k < V; ++k) {
                 const uint32_t p = q0 + k;
-                if (p < N32) {
-                    const uint32_t jb = k == 0 ? jm : j[k - 1];
-                    sS[p] = jb + E - p;
-                    if (j[k] == jb) {
-                        ep[E] = p;
-                        ++E;
-                    }
+                const uint32_t jb = k == 0 ? jm : j[k - 1];
+                sv[k] = jb + E - p;
+                if ((whole || p < N32) && j[k] == jb) {
+                    ep[E] = p;
+                    ++E;
                 }
+            }
+            if (whole) {
+                st8(sS + q0, sv);
+            } else {
+#pragma unroll
+                for (int k = 0; k < V; ++k)
+                    if (q0 + k < N32) sS[q0 + k] = sv[k];
             }
         }
         __syncthreads();
@@ -628,12 +674,22 @@ struct FilterRun {
                 uint32_t ss[V + 1];
                 R xv[V];
                 double xsv[V];
+                if (q0 + V <= N32) {
+                    uint32_t s8[V];
+                    ld8(sS + q0, s8);
 #pragma unroll
-                for (int k = 0; k <= V; ++k) ss[k] = q0 + k < N32 ? sS[q0 + k] : ne;
+                    for (int k = 0; k < V; ++k) ss[k] = s8[k];
+                    ss[V] = q0 + V < N32 ? sS[q0 + V] : ne;
+                    ld8(xc + q0, xv);
+                    if constexpr (SHADOW) ld8(xsc + q0, xsv);
+                } else {
 #pragma unroll
-                for (int k = 0; k < V; ++k) {
-                    xv[k] = q0 + k < N32 ? xc[q0 + k] : R(0);
-                    if constexpr (SHADOW) xsv[k] = q0 + k < N32 ? xsc[q0 + k] : 0.0;
+                    for (int k = 0; k <= V; ++k) ss[k] = q0 + k < N32 ? sS[q0 + k] : ne;
+#pragma unroll
+                    for (int k = 0; k < V; ++k) {
+                        xv[k] = q0 + k < N32 ? xc[q0 + k] : R(0);
+                        if constexpr (SHADOW) xsv[k] = q0 + k < N32 ? xsc[q0 + k] : 0.0;
+                    }
                 }
 #pragma unroll
                 for (int k = 0; k < V; ++k) {
