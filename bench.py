@@ -75,6 +75,11 @@ LOG2N = 28
 # two particles), ex2 for the weight; nominal 16 results / clock / SM.
 MUFU_PER_PS = 3.0
 MUFU_PER_CLK_SM = 16
+# From the ncu capture summarised in profiles/k_pf_batched_c4.md: warp
+# instructions per particle-step of the batched kernel, and DRAM bytes per
+# particle-step (read + write), measured on a 2.4e8 particle-step case.
+WARP_INSTR_PER_PS = 10.13
+DRAM_BYTES_PER_PS = 13.5
 
 
 def measured_peaks():
@@ -649,7 +654,15 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic: AR(1) observations simulated from per-filter Philox4x32 seeds", "config": cfg,
             "roofline": {"bound": "mufu", "kernel": "k_pf_batched<float>", "achieved": achieved, "peak": peak,
-                         "unit": "Gop/s", "frac": achieved / peak, "traffic": None,
+                         "unit": "Gop/s", "frac": achieved / peak,
+                         "traffic": DRAM_BYTES_PER_PS * res["ps_per_step"],
+                         "traffic_note": "DRAM bytes per launch: ncu bytes per particle-step on a medium case x "
+                                         "particle-steps per launch (profiles/k_pf_batched_c4.md)",
+                         "issue_slots": {"achieved": res["value"] / world * WARP_INSTR_PER_PS / 1e9,
+                                         "peak": 148 * 4 * sm_max / 1e3, "unit": "G warp-instr/s",
+                                         "frac": res["value"] / world * WARP_INSTR_PER_PS / (148 * 4 * sm_max * 1e6),
+                                         "note": "the binding resource: ncu warp-instructions per particle-step x "
+                                                 "particle-steps/s against one issue per clock per SM sub-partition"},
                          "peak_kind": "nominal: 16 MUFU results/clk/SM x 148 SMs x clocks.max.sm (the measured "
                                       "peaks file has no MUFU figure)",
                          "at_sampled_clock_frac": achieved / (148 * MUFU_PER_CLK_SM * sm_mhz / 1e3),

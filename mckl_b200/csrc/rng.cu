@@ -119,8 +119,9 @@ __device__ __forceinline__ void store_aligned(R *p, const R (&v)[N])
         constexpr int Q = static_cast<int>(sizeof(R) * N / 16);
         const uint4 *src = reinterpret_cast<const uint4 *>(v);
         uint4 *dst = reinterpret_cast<uint4 *>(p);
+        // streaming stores: the output is written once and not read back here
 #pragma unroll
-        for (int q = 0; q < Q; ++q) dst[q] = src[q];
+        for (int q = 0; q < Q; ++q) __stcs(dst + q, src[q]);
     } else {
 #pragma unroll
         for (int q = 0; q < N; ++q) p[q] = v[q];
@@ -176,17 +177,26 @@ __global__ void __launch_bounds__(256) k_blocks(G g, Ctr base, uint64_t nblk, ty
     constexpr int WPB = G::kWords / WordView<W>::kPer32;  // words per block
     constexpr int OPB = WPB / F::kIn;                     // outputs per block
     g.prepare();
+    // two blocks per thread and iteration, a grid stride apart (each store
+    // instruction stays coalesced across the warp): independent work to
+    // overlap with the stores in flight
+    constexpr int U = 2;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    for (uint64_t b = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; b < nblk; b += stride) {
-        uint32_t blk[G::kWords];
-        g.block(ctr_add(base, b, G::kCtrWords), blk);
-        W w[WPB];
+    for (uint64_t b0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; b0 < nblk; b0 += U * stride) {
 #pragma unroll
-        for (int j = 0; j < WPB; ++j) w[j] = WordView<W>::get(blk, j);
-        R o[OPB];
+        for (int i = 0; i < U; ++i) {
+            const uint64_t b = b0 + i * stride;
+            if (b >= nblk) break;
+            uint32_t blk[G::kWords];
+            g.block(ctr_add(base, b, G::kCtrWords), blk);
+            W w[WPB];
 #pragma unroll
-        for (int j = 0; j < OPB; ++j) o[j] = f(w + j * F::kIn);
-        store_aligned<R, OPB>(out + b * OPB, o);
+            for (int j = 0; j < WPB; ++j) w[j] = WordView<W>::get(blk, j);
+            R o[OPB];
+#pragma unroll
+            for (int j = 0; j < OPB; ++j) o[j] = f(w + j * F::kIn);
+            store_aligned<R, OPB>(out + b * OPB, o);
+        }
     }
 }
 
