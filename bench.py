@@ -483,6 +483,18 @@ def bench_rng(rank, world, dev, steps, warmup, e2e=True, clocks_on=True):
         torch.cuda.synchronize()
         ms = a.elapsed_time(bb) / reps
         c1[name] = {"ms": round(ms, 4), "GB_s": round(nbytes / (ms / 1e3) / 1e9, 1)}
+    # the device's write bandwidth on the same size: a store-only kernel
+    # (torch fill_) writing the 2^26 words, same repetitions
+    a, bb = events()
+    for _ in range(3):
+        p32.fill_(1)
+    a.record(stream)
+    for _ in range(50):
+        p32.fill_(1)
+    bb.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(bb) / 50
+    c1["store_only_fill_2^26"] = {"ms": round(ms, 4), "GB_s": round((4 << 26) / (ms / 1e3) / 1e9, 1)}
     out = dict(value=value, elapsed=elapsed, bytes_per_step=bytes_per_step, per_op=per_op, clocks=clk,
                launches=launches, philox_c1=c1)
     if e2e:
@@ -679,9 +691,11 @@ def main():
                            "per_op": {k: {"ms": round(v["ms"], 4), "GB_s": round(v["GB_s"], 1)}
                                       for k, v in rng["per_op"].items()},
                            "philox4x32_config": rng["philox_c1"],
-                           "roofline": {"bound": "hbm", "kernel": "k_blocks<PhiloxGen> (2^26 raw words)",
+                           "roofline": {"bound": "hbm", "kernel": "k_blocks<PhiloxGenRK> (2^26 raw words)",
                                         "achieved": ph, "peak": hbm_peak, "unit": "GB/s",
-                                        "peak_kind": f"{peak_kind} hbm_gbs", "frac": ph / hbm_peak}}
+                                        "peak_kind": f"{peak_kind} hbm_gbs", "frac": ph / hbm_peak,
+                                        "frac_of_store_only_fill":
+                                            ph / rng["philox_c1"]["store_only_fill_2^26"]["GB_s"]}}
             if rank == 0 and world == 1:
                 cb = cpu_smc_reference(res["w"], args.obs, 128)
                 if cb:

@@ -691,21 +691,35 @@ struct FilterRun {
                         if constexpr (SHADOW) xsv[k] = q0 + k < N32 ? xsc[q0 + k] : 0.0;
                     }
                 }
+                // the group's copies are the empties ep[ss[0], ss[V]), parent
+                // k owning [ss[k], ss[k+1]); heavy parents go to the queue
+                uint32_t heavy = 0;
 #pragma unroll
                 for (int k = 0; k < V; ++k) {
-                    const uint32_t s0 = ss[k], s1 = ss[k + 1];
-                    if (q0 + k >= N32 || s1 <= s0) continue;
-                    if (s1 - s0 > 32) {
+                    if (q0 + k < N32 && ss[k + 1] - ss[k] > 32) {
                         const uint32_t q = atomicAdd(nbig, 1u);
                         if (q < kBigParents) {
                             big[q] = q0 + k;
-                            continue;
+                            heavy |= 1u << k;
                         }
                     }
-                    for (uint32_t c = s0; c < s1; ++c) {
-                        const uint32_t e = ep[c];
-                        xc[e] = xv[k];
-                        if constexpr (SHADOW) xsc[e] = xsv[k];
+                }
+                // eight empties at a time: their slots are loaded together,
+                // then each takes its parent's particle
+                for (uint32_t cb = ss[0]; cb < ss[V]; cb += 8) {
+                    uint32_t e[8];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) e[i] = cb + i < ss[V] ? ep[cb + i] : 0u;
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        const uint32_t c = cb + i;
+                        if (c >= ss[V]) break;
+                        int k = 0;
+#pragma unroll
+                        for (int q = 1; q < V; ++q) k += ss[q] <= c ? 1 : 0;
+                        if (heavy & (1u << k)) continue;
+                        xc[e[i]] = xv[k];
+                        if constexpr (SHADOW) xsc[e[i]] = xsv[k];
                     }
                 }
             }

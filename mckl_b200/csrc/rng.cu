@@ -571,8 +571,8 @@ int mckl_b200_philox4x32_kernel(uint64_t ctr[2], size_t n, void *r, const uint32
     MB_CHECK_ARG(n == 0 || r != nullptr, "null output");
     Ctr B{{ctr[0], ctr[1], 0, 0}};
     B = ctr_add(B, 1, 2);
-    PhiloxGen g{key[0], key[1]};
-    int rc = launch_words<PhiloxGen, uint32_t>(g, B, 0, n * 4, static_cast<uint32_t *>(r), RawOut<uint32_t>{},
+    PhiloxGenRK g = PhiloxGenRK::make(key[0], key[1]);
+    int rc = launch_words<PhiloxGenRK, uint32_t>(g, B, 0, n * 4, static_cast<uint32_t *>(r), RawOut<uint32_t>{},
         as_stream(stream));
     if (rc != MCKL_B200_OK) return rc;
     Ctr E = ctr_add(Ctr{{ctr[0], ctr[1], 0, 0}}, n, 2);
