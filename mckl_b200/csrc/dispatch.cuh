@@ -46,7 +46,7 @@ inline int with_generator(const mckl_b200_engine_t &e, Fn &&fn)
     switch (e.kind) {
         case MCKL_B200_PHILOX4X32:
         case MCKL_B200_PHILOX4X32_64: {
-            PhiloxGenRK g = PhiloxGenRK::make(static_cast<uint32_t>(e.key[0]), static_cast<uint32_t>(e.key[1]));
+            PhiloxGen g{static_cast<uint32_t>(e.key[0]), static_cast<uint32_t>(e.key[1])};
             return fn(g);
         }
         case MCKL_B200_THREEFRY4X64:

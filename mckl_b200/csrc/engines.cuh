@@ -59,58 +59,16 @@ struct PhiloxGen {
         uint32_t a = k0, b = k1;
 #pragma unroll
         for (int r = 0; r < 10; ++r) {
-            const uint64_t p2 = static_cast<uint64_t>(s2) * 0xCD9E8D57u;  // one wide multiply
-            const uint64_t p0 = static_cast<uint64_t>(s0) * 0xD2511F53u;
-            s0 = a ^ s1 ^ static_cast<uint32_t>(p2 >> 32);
-            s1 = static_cast<uint32_t>(p2);
-            s2 = b ^ s3 ^ static_cast<uint32_t>(p0 >> 32);
-            s3 = static_cast<uint32_t>(p0);
+            const uint32_t hi2 = __umulhi(s2, 0xCD9E8D57u);
+            const uint32_t lo2 = s2 * 0xCD9E8D57u;
+            const uint32_t hi0 = __umulhi(s0, 0xD2511F53u);
+            const uint32_t lo0 = s0 * 0xD2511F53u;
+            s0 = a ^ s1 ^ hi2;
+            s1 = lo2;
+            s2 = b ^ s3 ^ hi0;
+            s3 = lo0;
             a += 0x9E3779B9u;
             b += 0xBB67AE85u;
-        }
-        out[0] = s0;
-        out[1] = s1;
-        out[2] = s2;
-        out[3] = s3;
-    }
-};
-
-// Philox4x32-10 with the ten round keys computed once on the host: in the
-// fill kernels they are kernel parameters, read by the xors straight from
-// the constant bank, so a round is two wide multiplies and two xors.  Same
-// stream as PhiloxGen.
-struct PhiloxGenRK {
-    static constexpr int kWords = 4;
-    static constexpr int kCtrWords = 2;
-    static constexpr int kDynSmem = 0;
-    uint32_t rk[10][2];
-
-    __host__ static PhiloxGenRK make(uint32_t k0, uint32_t k1)
-    {
-        PhiloxGenRK g;
-        for (int r = 0; r < 10; ++r) {
-            g.rk[r][0] = k0 + 0x9E3779B9u * static_cast<uint32_t>(r);
-            g.rk[r][1] = k1 + 0xBB67AE85u * static_cast<uint32_t>(r);
-        }
-        return g;
-    }
-
-    __device__ __forceinline__ void prepare() const {}
-
-    __device__ __forceinline__ void block(const Ctr &c, uint32_t out[4]) const
-    {
-        uint32_t s0 = static_cast<uint32_t>(c.w[0]);
-        uint32_t s1 = static_cast<uint32_t>(c.w[0] >> 32);
-        uint32_t s2 = static_cast<uint32_t>(c.w[1]);
-        uint32_t s3 = static_cast<uint32_t>(c.w[1] >> 32);
-#pragma unroll
-        for (int r = 0; r < 10; ++r) {
-            const uint64_t p2 = static_cast<uint64_t>(s2) * 0xCD9E8D57u;
-            const uint64_t p0 = static_cast<uint64_t>(s0) * 0xD2511F53u;
-            s0 = rk[r][0] ^ s1 ^ static_cast<uint32_t>(p2 >> 32);
-            s1 = static_cast<uint32_t>(p2);
-            s2 = rk[r][1] ^ s3 ^ static_cast<uint32_t>(p0 >> 32);
-            s3 = static_cast<uint32_t>(p0);
         }
         out[0] = s0;
         out[1] = s1;

@@ -177,10 +177,10 @@ __global__ void __launch_bounds__(256) k_blocks(G g, Ctr base, uint64_t nblk, ty
     constexpr int WPB = G::kWords / WordView<W>::kPer32;  // words per block
     constexpr int OPB = WPB / F::kIn;                     // outputs per block
     g.prepare();
-    // two blocks per thread and iteration, a grid stride apart (each store
+    // four blocks per thread and iteration, a grid stride apart (each store
     // instruction stays coalesced across the warp): independent work to
     // overlap with the stores in flight
-    constexpr int U = 2;
+    constexpr int U = 4;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t b0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; b0 < nblk; b0 += U * stride) {
 #pragma unroll
@@ -571,8 +571,8 @@ int mckl_b200_philox4x32_kernel(uint64_t ctr[2], size_t n, void *r, const uint32
     MB_CHECK_ARG(n == 0 || r != nullptr, "null output");
     Ctr B{{ctr[0], ctr[1], 0, 0}};
     B = ctr_add(B, 1, 2);
-    PhiloxGenRK g = PhiloxGenRK::make(key[0], key[1]);
-    int rc = launch_words<PhiloxGenRK, uint32_t>(g, B, 0, n * 4, static_cast<uint32_t *>(r), RawOut<uint32_t>{},
+    PhiloxGen g{key[0], key[1]};
+    int rc = launch_words<PhiloxGen, uint32_t>(g, B, 0, n * 4, static_cast<uint32_t *>(r), RawOut<uint32_t>{},
         as_stream(stream));
     if (rc != MCKL_B200_OK) return rc;
     Ctr E = ctr_add(Ctr{{ctr[0], ctr[1], 0, 0}}, n, 2);
