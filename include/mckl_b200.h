@@ -229,6 +229,14 @@ int mckl_b200_batched_run_graph(mckl_b200_batched_t *b, void *stream);
 int mckl_b200_batched_results(mckl_b200_batched_t *b, double *loglik, uint32_t *nresampled, void *stream);
 int mckl_b200_batched_shadow(mckl_b200_batched_t *b, double *loglik_fp64, void *stream);
 /* Replace the observations (HOST array of F x (T + 1), copied on `stream`). */
+/* New parameters / new keys for every filter of a handle (HOST arrays of F,
+ * keys F x 2), copied on `stream`; the next run (graph replays included)
+ * uses them.  For callers that rerun the same filters with other parameters
+ * or fresh randomness, e.g. the PMCMC driver below. */
+int mckl_b200_batched_set_params(mckl_b200_batched_t *b, const double *phi, const double *sx, const double *sy,
+                                 void *stream);
+int mckl_b200_batched_set_keys(mckl_b200_batched_t *b, const uint32_t *mkeys, const uint32_t *rkeys, void *stream);
+
 /* Shadow-run parameters (handles created with fp64 = 2 or 3): the FP64 shadow
  * follows the main run's resampling decisions and parent indices with its own
  * (phi, sx, sy) per filter (host arrays of F).  With perturbed parameters it
@@ -265,6 +273,25 @@ int mckl_b200_batched_destroy(mckl_b200_batched_t *b);
  * (nullable) receives every s_i; *final_value (host) the last.  Synchronizes. */
 int mckl_b200_fold_f64(size_t n, const double *x_dev, double s0, double *prefix_dev, double *final_value,
     void *stream);
+
+/* ---- PMCMC: PMCMCMutation (algorithm/pmcmc.hpp:72-165) ----------------
+ * C particle marginal Metropolis-Hastings chains of the AR(1) model, one
+ * batched filter per chain and iteration.  Chain c starts at theta0[3c..]
+ * = (phi, sx, sy), proposes theta + step * z (z standard normal, symmetric
+ * random walk) and accepts when log(U01) < -prior(theta) - logL(theta) +
+ * prior(theta') + logL(theta'), the reference's order of terms.  `prior`
+ * returns the log prior density (-inf outside the support; proposals with
+ * |phi| >= 1 or a non-positive scale are rejected without a filter run).
+ * Randomness: proposals and uniforms from Philox4x32 key (seed, c) at
+ * counters 2i and 2i + 1; filter keys (c, mix(seed, 2i)) and
+ * (c, mix(seed, 2i + 1)).  Outputs (HOST): theta_out iters x C x 3,
+ * loglik_out iters x C (state after each iteration; iteration 0 is the
+ * start), accepted C.  fp64: 0 FP32 moves (the chosen form), 1 FP64. */
+typedef double (*mckl_b200_log_prior_t)(const double *theta, void *user);
+int mckl_b200_pmcmc_ar1(size_t C, const size_t *N, size_t T, const double *y, const double *theta0,
+                        const double *step, mckl_b200_log_prior_t prior, void *user, size_t iters, uint32_t seed,
+                        int fp64, double threshold, double *theta_out, double *loglik_out, uint32_t *accepted,
+                        void *stream);
 
 /* ---- diagnostics (no counterpart in the reference) ----------------------
  * The library's double-double log (fn 0), exp (fn 1) and sin/cos (fn 2; cos

@@ -193,6 +193,11 @@ _bt_set_y = _bind("mckl_b200_batched_set_y", [_vp, _vp, _vp])
 _bt_autotune = _bind("mckl_b200_batched_autotune", [_vp, _i, _vp, _vp, _vp, _vp, _vp])
 _bt_shadow_params = _bind("mckl_b200_batched_shadow_params", [_vp, _vp, _vp, _vp])
 _bt_adjoint = _bind("mckl_b200_batched_adjoint", [_vp, _i, _vp, _vp, _vp])
+_bt_set_params = _bind("mckl_b200_batched_set_params", [_vp, _vp, _vp, _vp, _vp])
+_bt_set_keys = _bind("mckl_b200_batched_set_keys", [_vp, _vp, _vp, _vp])
+_LOG_PRIOR = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p)
+_pmcmc = _bind("mckl_b200_pmcmc_ar1", [_sz, _vp, _sz, _vp, _vp, _vp, _LOG_PRIOR, _vp, _sz, ctypes.c_uint32, _i,
+                                       _d, _vp, _vp, _vp, _vp])
 
 
 def _arr(a, dt):
@@ -254,6 +259,17 @@ class BatchedFilters:
                            g.ctypes.data_as(ctypes.c_void_p), _stream_ptr(stream)))
         return ll, g
 
+    def set_params(self, phi, sx, sy, stream=None):
+        """New (phi, sx, sy) for every filter; the next run uses them."""
+        a = [_arr(v, np.float64) for v in (phi, sx, sy)]
+        _check(_bt_set_params(self.h, *[v.ctypes.data_as(ctypes.c_void_p) for v in a], _stream_ptr(stream)))
+
+    def set_keys(self, mkeys, rkeys, stream=None):
+        """New model / resampling keys ([F, 2] each) for every filter."""
+        m, r = _arr(mkeys, np.uint32), _arr(rkeys, np.uint32)
+        _check(_bt_set_keys(self.h, m.ctypes.data_as(ctypes.c_void_p), r.ctypes.data_as(ctypes.c_void_p),
+                            _stream_ptr(stream)))
+
     def set_y(self, y, stream=None):
         """Copy new observations (host array [F, T + 1]; page-locked for an async copy)."""
         ptr = y.data_ptr() if hasattr(y, "data_ptr") else np.ascontiguousarray(y, dtype=np.float64).ctypes.data
@@ -307,6 +323,35 @@ def batched_workload(F=4096, T=500, seed=1234, nmin=256, nmax=65536):
     mkeys = np.stack([np.arange(F), np.full(F, 11)], axis=1).astype(np.uint32)
     rkeys = np.stack([np.arange(F), np.full(F, 12)], axis=1).astype(np.uint32)
     return dict(N=N, y=y, phi=phi, sx=sx, sy=sy, sd0=sd0, mkeys=mkeys, rkeys=rkeys)
+
+
+def pmcmc_ar1(y, N, theta0, step, log_prior, iters, seed=1, fp64=False, threshold=0.5):
+    """Particle marginal Metropolis-Hastings, C chains at once
+    (mckl_b200_pmcmc_ar1).  y: [C, T + 1] (or [T + 1], shared); N: particles
+    per chain (int or [C]); theta0: [C, 3] = (phi, sx, sy); step: random-walk
+    scales [3]; log_prior(theta) -> float.  Returns (theta [iters, C, 3],
+    loglik [iters, C], accepted [C])."""
+    theta0 = _arr(np.atleast_2d(theta0), np.float64)
+    C = theta0.shape[0]
+    y = np.asarray(y, dtype=np.float64)
+    if y.ndim == 1:
+        y = np.broadcast_to(y, (C, y.shape[0]))
+    y = _arr(y, np.float64)
+    T = y.shape[1] - 1
+    Nv = _arr(np.broadcast_to(np.asarray(N, dtype=np.uint64), (C,)), np.uint64)
+    st = _arr(step, np.float64)
+    th = np.zeros((iters, C, 3))
+    ll = np.zeros((iters, C))
+    acc = np.zeros(C, dtype=np.uint32)
+
+    def _prior(p, _user):
+        return float(log_prior(np.array([p[0], p[1], p[2]])))
+
+    cb = _LOG_PRIOR(_prior)
+    vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    _check(_pmcmc(C, vp(Nv), T, vp(y), vp(theta0), vp(st), cb, None, iters, seed & 0xFFFFFFFF, int(bool(fp64)),
+                  threshold, vp(th), vp(ll), vp(acc), _stream_ptr()))
+    return th, ll, acc
 
 
 def fold_f64(x, s0: float = 0.0, prefix=True):

@@ -1151,6 +1151,17 @@ using namespace mckl_b200;
 
 namespace {
 
+// main-run parameters of one filter and their derived constants
+void set_main(BatchedFilter &h, double phi, double sx, double sy)
+{
+    h.phi = phi;
+    h.sx = sx;
+    h.sd0 = sx / std::sqrt(1 - phi * phi);
+    h.lconst = -std::log(sy) - 0.5 * std::log(2 * 3.14159265358979323846);
+    h.hinv = 0.5 / (sy * sy);
+    h.sy = sy;
+}
+
 // shadow-run parameters of one filter (the same derived constants as the main run's)
 void set_shadow(BatchedFilter &h, double phi, double sx, double sy)
 {
@@ -1178,12 +1189,7 @@ int mckl_b200_batched_create(mckl_b200_batched_t **out, size_t F, const size_t *
         MB_CHECK_ARG(sy[f] > 0 && phi[f] * phi[f] < 1, "need sy > 0 and |phi| < 1");
         h[f].n = N[f];
         h[f].off = total;
-        h[f].phi = phi[f];
-        h[f].sx = sx[f];
-        h[f].sd0 = sx[f] / std::sqrt(1 - phi[f] * phi[f]);
-        h[f].lconst = -std::log(sy[f]) - 0.5 * std::log(2 * 3.14159265358979323846);
-        h[f].hinv = 0.5 / (sy[f] * sy[f]);
-        h[f].sy = sy[f];
+        set_main(h[f], phi[f], sx[f], sy[f]);
         set_shadow(h[f], phi[f], sx[f], sy[f]);
         h[f].mkey[0] = mkeys[2 * f];
         h[f].mkey[1] = mkeys[2 * f + 1];
@@ -1382,6 +1388,36 @@ int mckl_b200_batched_shadow_params(mckl_b200_batched_t *b, const double *phi, c
         set_shadow(b->hf[f], phi[f], sx[f], sy[f]);
     }
     MB_CUDA(cudaMemcpy(b->a.filt, b->hf.data(), b->hf.size() * sizeof(BatchedFilter), cudaMemcpyHostToDevice));
+    return MCKL_B200_OK;
+}
+
+int mckl_b200_batched_set_params(mckl_b200_batched_t *b, const double *phi, const double *sx, const double *sy,
+    void *stream)
+{
+    MB_CHECK_ARG(b != nullptr && phi && sx && sy, "null argument");
+    for (int f = 0; f < b->F; ++f) {
+        MB_CHECK_ARG(sy[f] > 0 && phi[f] * phi[f] < 1, "need sy > 0 and |phi| < 1");
+    }
+    for (int f = 0; f < b->F; ++f) {
+        set_main(b->hf[f], phi[f], sx[f], sy[f]);
+        set_shadow(b->hf[f], phi[f], sx[f], sy[f]);
+    }
+    MB_CUDA(cudaMemcpyAsync(b->a.filt, b->hf.data(), b->hf.size() * sizeof(BatchedFilter), cudaMemcpyHostToDevice,
+        as_stream(stream)));
+    return MCKL_B200_OK;
+}
+
+int mckl_b200_batched_set_keys(mckl_b200_batched_t *b, const uint32_t *mkeys, const uint32_t *rkeys, void *stream)
+{
+    MB_CHECK_ARG(b != nullptr && mkeys && rkeys, "null argument");
+    for (int f = 0; f < b->F; ++f) {
+        b->hf[f].mkey[0] = mkeys[2 * f];
+        b->hf[f].mkey[1] = mkeys[2 * f + 1];
+        b->hf[f].rkey[0] = rkeys[2 * f];
+        b->hf[f].rkey[1] = rkeys[2 * f + 1];
+    }
+    MB_CUDA(cudaMemcpyAsync(b->a.filt, b->hf.data(), b->hf.size() * sizeof(BatchedFilter), cudaMemcpyHostToDevice,
+        as_stream(stream)));
     return MCKL_B200_OK;
 }
 
