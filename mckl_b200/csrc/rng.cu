@@ -139,6 +139,7 @@ template <typename W>
 struct RawOut {
     using out_t = W;
     static constexpr int kIn = 1;
+    static constexpr bool kCheap = true;
     __device__ W operator()(const W *w) const { return w[0]; }
 };
 
@@ -146,6 +147,7 @@ template <typename R, typename W>
 struct U01Out {
     using out_t = R;
     static constexpr int kIn = 1;
+    static constexpr bool kCheap = true;
     int variant;
     __device__ R operator()(const W *w) const { return RealOps<R>::u01(variant, w[0]); }
 };
@@ -153,6 +155,7 @@ struct U01Out {
 struct Canon2Out {
     using out_t = double;
     static constexpr int kIn = 2;
+    static constexpr bool kCheap = true;
     __device__ double operator()(const uint32_t *w) const { return u01_canonical2(w[0], w[1]); }
 };
 
@@ -160,6 +163,7 @@ template <typename R, typename W>
 struct ExpOut {
     using out_t = R;
     static constexpr int kIn = 1;
+    static constexpr bool kCheap = false;
     R a;  // -1 / lambda, rounded in R as the reference does
     __device__ R operator()(const W *w) const
     {
@@ -179,8 +183,9 @@ __global__ void __launch_bounds__(256) k_blocks(G g, Ctr base, uint64_t nblk, ty
     g.prepare();
     // four blocks per thread and iteration, a grid stride apart (each store
     // instruction stays coalesced across the warp): independent work to
-    // overlap with the stores in flight
-    constexpr int U = 4;
+    // overlap with the stores in flight; one for the transforms whose
+    // per-value math (double-double log) needs the registers
+    constexpr int U = F::kCheap ? 4 : 1;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t b0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; b0 < nblk; b0 += U * stride) {
 #pragma unroll
