@@ -290,6 +290,104 @@ def bench_smc(args, rank, world, dev):
     return out
 
 
+def bench_callers(dev, hbm_peak, peak_kind, reps=5):
+    """The callers either side of the filters: ResampleIndex's index matrix
+    (N = 2^20 particles, R = 100 iterations of parent indices from systematic
+    resampling of log-normal weights), SMCEstimator's weighted estimate
+    (n = 2^24 particles, d = 4) and the PMCMC caller (64 chains, N = 4096,
+    T = 200, 10 iterations).  Device-timed with CUDA events; algorithmic
+    bytes: the index matrix reads one parent word per entry and writes one
+    (2 x 8 B x N x R), the estimate reads u and W once (8 B x n x (d + 1))."""
+    import numpy as np
+    import torch
+
+    import mckl_b200 as mb
+
+    out = {}
+    stream = torch.cuda.current_stream()
+    N, R = 1 << 20, 100
+    g = torch.Generator(device="cuda").manual_seed(11)
+    rr = mb.Philox4x32(77)
+    ri = mb.ResampleIndex()
+    for _ in range(R):
+        W = torch.exp(torch.randn(N, dtype=torch.float64, device="cuda", generator=g))
+        W /= W.sum()
+        ri.push_back(N, mb.rep_to_index(mb.resample(mb.Systematic, rr, W), N))
+    for name, layout in (("col_major", ri.ColMajor), ("row_major", ri.RowMajor)):
+        for _ in range(2):
+            ri.index_matrix(layout)
+        torch.cuda.synchronize()
+        t0, t1 = events()
+        t0.record(stream)
+        for _ in range(reps):
+            ri.index_matrix(layout)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        ms = t0.elapsed_time(t1) / reps
+        gbs = 2 * 8 * N * R / ms / 1e6
+        out[f"index_matrix_{name}"] = {"ms": round(ms, 4), "GB_s": round(gbs, 1),
+                                       "frac_of_hbm": round(gbs / hbm_peak, 3)}
+    out["index_matrix_workload"] = f"N = 2^20, R = {R}, one launch + its error-flag read per call"
+    del ri
+    n, d = 1 << 24, 4
+    W = torch.rand(n, dtype=torch.float64, device="cuda", generator=g)
+    W /= W.sum()
+    for name, col in (("row_major", False), ("col_major", True)):
+        u = torch.randn((d, n) if col else (n, d), dtype=torch.float64, device="cuda", generator=g)
+        for _ in range(2):
+            mb.weighted_estimate(u, W, col_major=col)
+        torch.cuda.synchronize()
+        t0, t1 = events()
+        t0.record(stream)
+        for _ in range(reps):
+            mb.weighted_estimate(u, W, col_major=col)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        ms = t0.elapsed_time(t1) / reps
+        gbs = 8 * n * (d + 1) / ms / 1e6
+        out[f"weighted_estimate_{name}"] = {"ms": round(ms, 4), "GB_s": round(gbs, 1),
+                                            "frac_of_hbm": round(gbs / hbm_peak, 3)}
+        del u
+    out["weighted_estimate_workload"] = "n = 2^24, d = 4, FP64; inputs 671 MB, above the 126 MB L2"
+    out["hbm_peak"] = {"GB_s": hbm_peak, "kind": peak_kind}
+    C, Np, T, iters = 64, 4096, 200, 10
+    y = np.concatenate([[0.0], np.cumsum(np.random.default_rng(3).normal(size=T)) * 0.3])
+    theta0 = np.tile([0.9, 1.0, 0.5], (C, 1))
+    prior = lambda th: 0.0 if (abs(th[0]) < 1 and th[1] > 0 and th[2] > 0) else -np.inf  # noqa: E731
+    mb.pmcmc_ar1(y, Np, theta0, [0.02, 0.05, 0.05], prior, 2, seed=5)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    mb.pmcmc_ar1(y, Np, theta0, [0.02, 0.05, 0.05], prior, iters, seed=6)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t
+    out["pmcmc"] = {"chains": C, "N": Np, "T": T, "iterations": iters, "s": round(dt, 4),
+                    "chain_iterations_per_s": round(C * iters / dt, 1),
+                    "particle_steps_per_s": C * iters * Np * T / dt,
+                    "note": "wall clock (host prior callback and accept step between filter launches)"}
+    return out
+
+
+def cpu_callers_reference():
+    """The compiled reference's ResampleIndex::read_index_matrix (one thread)
+    on N = 2^16, R = 100 (push_back copies included)."""
+    import numpy as np
+
+    import oracle as O
+
+    if not O.have_ref():
+        return None
+    cpu = O.CPUPath("ref")
+    N, R = 1 << 16, 100
+    idx = np.random.default_rng(1).integers(0, N, size=(R, N)).astype(np.uint64)
+    outm = np.zeros(N * R, dtype=np.uint64)
+    t = time.perf_counter()
+    cpu._index_matrix(N, R, idx.ctypes.data_as(ctypes.c_void_p), R - 1, 0, 1,
+                      outm.ctypes.data_as(ctypes.c_void_p), None)
+    dt = time.perf_counter() - t
+    return {"index_matrix_GB_s": 2 * 8 * N * R / dt / 1e9, "cores": 1, "kind": "reference",
+            "sample": "N = 2^16, R = 100 random parents, column-major"}
+
+
 def bench_adjoint(rank, dev, sets=256, N=1 << 16, T=1000, C=32, threads=512):
     """Differentiated SMC: gradient of the FP64 estimate in (phi, sx, sy) for
     `sets` parameter sets drawn like the batched workload, N particles, T
@@ -699,7 +797,12 @@ def main():
                                         "peak_kind": f"{peak_kind} hbm_gbs", "frac": ph / hbm_peak,
                                         "frac_of_store_only_fill":
                                             ph / rng["philox_c1"]["store_only_fill_2^26"]["GB_s"]}}
+            if rank == 0:
+                line["callers"] = bench_callers(dev, hbm_peak, peak_kind)
             if rank == 0 and world == 1:
+                cc = cpu_callers_reference()
+                if cc:
+                    line["callers"]["cpu_reference"] = cc
                 cb = cpu_smc_reference(res["w"], args.obs, 128)
                 if cb:
                     line["cpu_baseline"] = strip(cb)

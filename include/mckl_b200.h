@@ -274,6 +274,38 @@ int mckl_b200_batched_destroy(mckl_b200_batched_t *b);
 int mckl_b200_fold_f64(size_t n, const double *x_dev, double s0, double *prefix_dev, double *final_value,
     void *stream);
 
+/* ---- Engine state in the reference's text form --------------------------
+ * CounterEngine's operator<< / operator>> (random/counter.hpp:235-272): save
+ * writes the text `os << eng` produces for the engine in this state
+ * (buffered results, counter, generator parameters, index; an unused buffer
+ * as zeros) into buf (cap bytes; *len = its length, buf == NULL only asks
+ * for it); load parses such text into *e of the given kind and checks the
+ * buffered results against the counter.  Host-only, no device work. */
+int mckl_b200_engine_save(const mckl_b200_engine_t *e, char *buf, size_t cap, size_t *len);
+int mckl_b200_engine_load(mckl_b200_engine_t *e, uint32_t kind, const char *text);
+
+/* ---- Genealogy: ResampleIndex (algorithm/resample.hpp:597-832) ----------
+ * The ancestors of the N particles of the last of R recorded iterations at
+ * every one of the R iterations (ResampleIndex::read_index_matrix, :752-829):
+ * index_host is a HOST array of R DEVICE pointers to uint64 parent-index
+ * vectors (entry r of sizes_host entries; the last has N), oldest first;
+ * out (DEVICE) is N x R, row-major (R per particle) or column-major.  One
+ * thread follows each particle's line back.  A parent index outside the
+ * previous vector returns MCKL_B200_ERR_ARG.  Synchronizes the stream (to
+ * read the error word). */
+int mckl_b200_index_matrix(size_t N, size_t R, const uint64_t *const *index_host, const size_t *sizes_host,
+                           int col_major, uint64_t *out_dev, void *stream);
+
+/* ---- Estimates: SMCEstimator::estimate (algorithm/smc.hpp:90-120) -------
+ * result_j = sum_i W_i u(i, j), j < d: the reference's cblas_dgemv of the
+ * evaluations with the normalised weights.  u (DEVICE) n x d, row-major (d
+ * values per particle, the reference's RowMajor) or column-major; W and
+ * result DEVICE.  Deterministic order: FP64 partial sums over fixed ranges of
+ * particles, then the partials in a fixed tree.  d <= 65535 column-major,
+ * d <= 65535 * 256 row-major. */
+int mckl_b200_weighted_estimate(size_t n, size_t d, int col_major, const double *u_dev, const double *W_dev,
+                                double *result_dev, void *stream);
+
 /* ---- PMCMC: PMCMCMutation (algorithm/pmcmc.hpp:72-165) ----------------
  * C particle marginal Metropolis-Hastings chains of the AR(1) model, one
  * batched filter per chain and iteration.  Chain c starts at theta0[3c..]

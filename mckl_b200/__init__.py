@@ -87,6 +87,8 @@ _exponential = {"f32": _bind("mckl_b200_exponential_f32", [_EP, _sz, _vp, _f, _v
                 "f64": _bind("mckl_b200_exponential_f64", [_EP, _sz, _vp, _d, _vp])}
 _gamma = {"f32": _bind("mckl_b200_gamma_f32", [_EP, _sz, _vp, _f, _f, _vp]),
           "f64": _bind("mckl_b200_gamma_f64", [_EP, _sz, _vp, _d, _d, _vp])}
+_engine_save = _bind("mckl_b200_engine_save", [_EP, ctypes.c_char_p, _sz, ctypes.POINTER(_sz)])
+_engine_load = _bind("mckl_b200_engine_load", [_EP, _u32, ctypes.c_char_p])
 _gamma_blocks = {"f32": _bind("mckl_b200_gamma_blocks_f32", [_EP, _sz, _sz, _vp, _d, _vp, _vp]),
                  "f64": _bind("mckl_b200_gamma_blocks_f64", [_EP, _sz, _sz, _vp, _d, _vp, _vp])}
 
@@ -325,6 +327,88 @@ def batched_workload(F=4096, T=500, seed=1234, nmin=256, nmax=65536):
     return dict(N=N, y=y, phi=phi, sx=sx, sy=sy, sd0=sd0, mkeys=mkeys, rkeys=rkeys)
 
 
+_index_matrix = _bind("mckl_b200_index_matrix", [_sz, _sz, _vp, _vp, _i, _vp, _vp])
+_west = _bind("mckl_b200_weighted_estimate", [_sz, _sz, _i, _vp, _vp, _vp, _vp])
+
+
+def weighted_estimate(u, W, col_major=False):
+    """SMCEstimator's estimate: sum_i W_i u[i, :] (u: CUDA float64 [n, d],
+    or [d, n] with col_major)."""
+    torch = _torch()
+    u = u.contiguous()
+    n = W.numel()
+    if u.dim() == 2:
+        d = u.shape[0] if col_major else u.shape[1]
+    else:
+        d = u.numel() // max(n, 1)
+    if u.numel() != n * d or u.dtype != torch.float64 or W.dtype != torch.float64:
+        raise ValueError("u: float64 [n, d] (or [d, n] with col_major), W: float64 [n]")
+    out = torch.empty(d, dtype=torch.float64, device="cuda")
+    _check(_west(n, d, int(bool(col_major)), ctypes.c_void_p(u.data_ptr()), ctypes.c_void_p(W.data_ptr()),
+                 ctypes.c_void_p(out.data_ptr()), _stream_ptr()))
+    return out
+
+
+class ResampleIndex:
+    """mckl::ResampleIndex over parent-index vectors kept in device memory
+    (algorithm/resample.hpp:597-832): push_back, index, index_matrix."""
+
+    RowMajor, ColMajor = 0, 1
+
+    def __init__(self):
+        self._v = []
+
+    def num_iter(self):
+        return len(self._v)
+
+    def size(self, iter_=None):
+        if not self._v:
+            return 0
+        return int(self._v[-1 if iter_ is None else iter_].numel())
+
+    def reset(self):
+        self._v = []
+
+    def push_back(self, N, index=None):
+        """Append the parent indices of one iteration (a CUDA int64/uint64
+        tensor of N entries), or the identity when `index` is None."""
+        torch = _torch()
+        if index is None:
+            index = torch.arange(N, dtype=torch.int64, device="cuda")
+        if index.numel() != N or not index.is_cuda or index.element_size() != 8:
+            raise ValueError("index: CUDA tensor of N 64-bit integers")
+        self._v.append(index.contiguous())
+
+    def _run(self, vecs, col_major):
+        torch = _torch()
+        R = len(vecs)
+        N = int(vecs[-1].numel())
+        out = torch.empty(N * R, dtype=torch.int64, device="cuda")
+        ptrs = (ctypes.c_uint64 * R)(*[v.data_ptr() for v in vecs])
+        sizes = (ctypes.c_size_t * R)(*[v.numel() for v in vecs])
+        _check(_index_matrix(N, R, ctypes.cast(ptrs, _vp), ctypes.cast(sizes, _vp), int(col_major),
+                             ctypes.c_void_p(out.data_ptr()), _stream_ptr()))
+        return out
+
+    def index_matrix(self, layout=0, iter_back=None, iter_=0):
+        """N x R ancestors (flattened, row- or column-major) of iterations
+        iter_..iter_back, N the size at iter_back (:718-829)."""
+        ib = self.num_iter() - 1 if iter_back is None else iter_back
+        if not (0 <= iter_ <= ib < self.num_iter()):
+            raise IndexError("iteration numbers out of range")
+        return self._run(self._v[iter_:ib + 1], layout == self.ColMajor)
+
+    def index(self, id_, iter_back=None, iter_=0):
+        """index(id, iter_back, iter) (:666-678): from the last iteration's
+        vector, followed back through iterations iter_back - 1 .. iter_."""
+        ib = self.num_iter() - 1 if iter_back is None else iter_back
+        if not (0 <= iter_ <= ib < self.num_iter()):
+            raise IndexError("iteration numbers out of range")
+        vecs = self._v[iter_:ib] + [self._v[-1]]
+        col = self._run(vecs, True)
+        return int(col[id_].item())
+
+
 def pmcmc_ar1(y, N, theta0, step, log_prior, iters, seed=1, fp64=False, threshold=0.5):
     """Particle marginal Metropolis-Hastings, C chains at once
     (mckl_b200_pmcmc_ar1).  y: [C, T + 1] (or [T + 1], shared); N: particles
@@ -493,6 +577,26 @@ class CounterEngine:
     def state_tuple(self):
         s = self.state
         return (tuple(s.ctr), tuple(s.key), tuple(s.tweak), int(s.index), int(s.kind))
+
+    def __str__(self) -> str:
+        """The reference's ``os << rng`` text (random/counter.hpp:235-252)."""
+        n = _sz()
+        _check(_engine_save(ctypes.byref(self.state), None, 0, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value + 1)
+        _check(_engine_save(ctypes.byref(self.state), buf, n.value + 1, ctypes.byref(n)))
+        return buf.value.decode()
+
+    def load_text(self, text: str) -> None:
+        """The reference's ``is >> rng`` (random/counter.hpp:254-272); raises
+        on text that is not a state of this engine kind."""
+        _check(_engine_load(ctypes.byref(self.state), self.kind, text.encode()))
+
+    @classmethod
+    def from_text(cls, text: str):
+        e = cls.__new__(cls)
+        e.state = EngineState()
+        e.load_text(text)
+        return e
 
     def load_state(self, ctr, key, tweak, index) -> None:
         for i in range(4):

@@ -115,9 +115,14 @@ class CPUPath:
             f("block", [ep, vp, vp])
             f("math_f64", [i, sz, vp, vp, vp])
             f("fold", [sz, vp, d, vp, vp])
+            f("weighted_estimate", [sz, sz, i, vp, vp, vp])
         else:
             f("pf_ar1", [sz, sz, vp, d, d, d, d, vp, vp, i, d, i, vp, vp, vp, vp, vp, vp, i])
             f("pf_ar1_batch", [sz, vp, sz, vp, vp, vp, vp, vp, vp, i, d, vp, i])
+            f("index_matrix", [sz, sz, vp, sz, sz, i, vp, vp])
+            f("engine_to_text", [ep, ctypes.c_char_p, sz])
+            f("engine_from_text", [ep, ctypes.c_char_p])
+            f("engine_text_roundtrip", [ep, ctypes.c_char_p, ctypes.c_char_p, sz])
             f("fill_u32_parallel", [ep, sz, vp, i], restype=d)
             f("dist_parallel", [ep, i, i, sz, vp, i], restype=d)
             f("max_threads", [], restype=i)
@@ -203,6 +208,17 @@ class CPUPath:
         self._rep_index(len(rep), M, _ptr(rep), _ptr(idx))
         return idx[:M]
 
+    def weighted_estimate(self, u, W, col_major=False):
+        """SMCEstimator's estimate sum_i W_i u(i, j); u [n, d] (or [d, n]
+        with col_major)."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        W = np.ascontiguousarray(W, dtype=np.float64)
+        n = W.size
+        d = u.size // max(n, 1)
+        out = np.zeros(d)
+        self._weighted_estimate(n, d, int(bool(col_major)), _ptr(u), _ptr(W), _ptr(out))
+        return out
+
     def select_f64(self, idx, state):
         state = np.array(state, dtype=np.float64, order="F", copy=True)
         idx = np.ascontiguousarray(idx, dtype=np.uint64)
@@ -254,6 +270,36 @@ class CPUPath:
         fin = np.zeros(1)
         self._fold(len(x), _ptr(x), s0, _ptr(pre), _ptr(fin))
         return pre, float(fin[0])
+
+    def engine_text(self, eng):
+        """The reference's `os << eng` for an engine in state `eng`."""
+        buf = ctypes.create_string_buffer(4096)
+        e = eng.copy()
+        assert self._engine_to_text(ctypes.byref(e), buf, 4096) == 0
+        return buf.value.decode()
+
+    def engine_text_roundtrip(self, kind, text):
+        """`is >> eng` of `text`, then `os << eng`."""
+        buf = ctypes.create_string_buffer(4096)
+        e = Engine.make(kind)
+        assert self._engine_text_roundtrip(ctypes.byref(e), text.encode(), buf, 4096) == 0
+        return buf.value.decode()
+
+    def engine_from_text(self, kind, text):
+        """A state read by the reference's `is >> eng`."""
+        e = Engine.make(kind)
+        assert self._engine_from_text(ctypes.byref(e), text.encode()) == 0
+        return e
+
+    def index_matrix(self, idx, iter_back, iter_, col_major):
+        """ResampleIndex::read_index_matrix of R pushed vectors idx [R, N];
+        returns (matrix [N * R], trace of every id [N])."""
+        idx = np.ascontiguousarray(idx, dtype=np.uint64)
+        R, N = idx.shape
+        out = np.zeros(N * (iter_back - iter_ + 1), dtype=np.uint64)
+        tr = np.zeros(N, dtype=np.uint64)
+        assert self._index_matrix(N, R, _ptr(idx), iter_back, iter_, int(bool(col_major)), _ptr(out), _ptr(tr)) == 0
+        return out, tr
 
     def kalman_ar1(self, y, phi, sx, sy):
         y = np.ascontiguousarray(y, dtype=np.float64)

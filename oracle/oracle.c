@@ -719,6 +719,26 @@ int orc_pf_ar1(size_t N, size_t T, const double *y, double phi, double sx, doubl
     return 0;
 }
 
+/* SMCEstimator::estimate (algorithm/smc.hpp:100-117): result_j =
+ * sum_i W_i u(i, j) through cblas_dgemv (ColMajor NoTrans over the row-major
+ * evaluations, ColMajor Trans over the column-major ones).  The reference
+ * requires a BLAS (internal/cblas.hpp:75, 115-118), which fixes no summation
+ * order; this restates the order of the reference BLAS's dgemv loops (alpha =
+ * 1, beta = 0): a left fold over particles of the rounded products W_i u(i, j),
+ * the same in both layouts. */
+int orc_weighted_estimate(size_t n, size_t d, int col_major, const double *u, const double *w, double *out)
+{
+    for (size_t j = 0; j < d; ++j) {
+        double s = 0.0;
+        for (size_t i = 0; i < n; ++i) {
+            const double v = col_major ? u[j * n + i] : u[i * d + j];
+            s = s + w[i] * v;
+        }
+        out[j] = s;
+    }
+    return 0;
+}
+
 /* Sequential left fold s_i = s_{i-1} + x_i from s_{-1} = s0 (the
  * std::accumulate / `accw += w[i]` loops of core/weight.hpp:221 and
  * algorithm/resample.hpp:395-403); prefix may be NULL. */

@@ -57,6 +57,7 @@ int orc_pf_ar1(size_t N, size_t T, const double *y, double phi, double sx, doubl
     double sd0, const uint32_t mkey[2], const uint32_t rkey[2], int scheme,
     double threshold, double *loglik, double *ess_hist, uint8_t *resampled,
     uint64_t *anc, double *x_out, double *W_out);
+int orc_weighted_estimate(size_t n, size_t d, int col_major, const double *u, const double *w, double *out);
 int orc_fold(size_t n, const double *x, double s0, double *prefix, double *final_value);
 int orc_math_f64(int fn, size_t n, const double *x, double *y, double *y2);
 int orc_kalman_ar1(size_t T, const double *y, double phi, double sx, double sy,

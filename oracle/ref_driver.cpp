@@ -25,6 +25,7 @@
 // block, the key, the Threefry tweak, and the number of words of that block
 // already handed out (index == words per block means nothing is buffered).
 
+#include <cstring>
 #include <mckl/algorithm/resample.hpp>
 #include <mckl/algorithm/smc.hpp>
 #include <mckl/core/state_matrix.hpp>
@@ -468,6 +469,69 @@ int ref_rep_index(
     mckl::resample_trans_rep_index(N, M, r.data(), x.data());
     for (std::size_t i = 0; i != M; ++i) {
         idx[i] = x[i];
+    }
+    return 0;
+}
+
+// The engine in state `s` written with the reference's operator<<
+// (random/counter.hpp:235-250), and a state read with its operator>>
+// (:252-272) into `s`.
+int ref_engine_to_text(ref_engine *s, char *buf, std::size_t cap)
+{
+    std::string text;
+    with_engine(s, [&](auto &e) {
+        std::ostringstream os;
+        os << e;
+        text = os.str();
+    });
+    if (text.size() + 1 > cap) return 1;
+    std::memcpy(buf, text.c_str(), text.size() + 1);
+    return 0;
+}
+
+// Read `text` with operator>> and write the engine back with operator<<.
+int ref_engine_text_roundtrip(ref_engine *s, const char *text, char *buf, std::size_t cap)
+{
+    int rc = 0;
+    std::string out;
+    with_engine(s, [&](auto &e) {
+        std::istringstream is(text);
+        is >> e;
+        rc = is ? 0 : 1;
+        std::ostringstream os;
+        os << e;
+        out = os.str();
+    });
+    if (rc || out.size() + 1 > cap) return 1;
+    std::memcpy(buf, out.c_str(), out.size() + 1);
+    return 0;
+}
+
+int ref_engine_from_text(ref_engine *s, const char *text)
+{
+    int rc = 0;
+    with_engine(s, [&](auto &e) {
+        std::istringstream is(text);
+        is >> e;
+        rc = is ? 0 : 1;
+    });
+    return rc;
+}
+
+// ResampleIndex (algorithm/resample.hpp:597-832): push R parent-index
+// vectors of N entries, then read the ancestor matrix of iterations
+// iter..iter_back (row- or column-major) and the single-particle trace
+// index(id, iter_back, iter) for every id.
+int ref_index_matrix(std::size_t N, std::size_t R, const std::uint64_t *idx, std::size_t iter_back,
+    std::size_t iter, int col_major, std::uint64_t *out, std::uint64_t *trace)
+{
+    mckl::ResampleIndex<std::size_t> ri;
+    for (std::size_t r = 0; r < R; ++r) {
+        ri.push_back(N, idx + r * N);
+    }
+    ri.read_index_matrix(col_major ? mckl::ColMajor : mckl::RowMajor, out, iter_back, iter);
+    if (trace) {
+        for (std::size_t i = 0; i < N; ++i) trace[i] = ri.index(i, iter_back, iter);
     }
     return 0;
 }

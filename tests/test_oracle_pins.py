@@ -180,3 +180,27 @@ def test_kalman_gradient_vs_finite_differences(orc):
             lm, _ = orc.kalman_ar1(y, *p)
             fd = (lp - lm) / (2 * h)
             assert abs(fd - g[k]) <= 1e-6 * max(1.0, abs(fd)), (k, fd, g[k])
+
+
+def test_weighted_estimate_oracle_pin():
+    """The oracle's dgemv-order estimate against the exactly rounded sum
+    (math.fsum), within the FP64 error bound of an n-term sum, both layouts
+    identical; and against the installed BLAS's dgemv (any order) within the
+    same bound."""
+    import math
+
+    from scipy.linalg import blas
+
+    orc = O.CPUPath("oracle")
+    rng = np.random.default_rng(5)
+    for n, d in ((1, 1), (1000, 3), (5000, 17)):
+        W = rng.random(n)
+        W /= W.sum()
+        u = rng.normal(size=(n, d)) * 2 - 1
+        got = orc.weighted_estimate(u, W)
+        assert np.array_equal(got, orc.weighted_estimate(np.ascontiguousarray(u.T), W, col_major=True))
+        lib = blas.dgemv(1.0, u, W, trans=1)
+        for j in range(d):
+            bound = n * 2.0**-53 * float(np.sum(np.abs(W * u[:, j])))
+            assert abs(got[j] - math.fsum(W * u[:, j])) <= bound
+            assert abs(got[j] - lib[j]) <= 2 * bound
