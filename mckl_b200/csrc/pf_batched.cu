@@ -267,8 +267,25 @@ struct Step {
 // angle words of the block 128 further on, i.e. up to four pairs for two
 // Philox blocks (a quarter block per particle).  Units past the full chunks
 // are the pairs of the last partial chunk, drawn word by word.
-// Parents with many copies that the CTA copies together (per resampling).
+// Placement: a warp owns 32 x 8 consecutive parents per tile and copies them
+// into their empty slots; a warp with more than kWarpCopies copies in one tile
+// queues its parents (up to kBigParents queued groups) for the whole CTA.
 constexpr uint32_t kBigParents = 64;
+constexpr uint32_t kWarpParents = 256;
+constexpr uint32_t kWarpCopies = 512;
+constexpr uint32_t kWs = kWarpParents + 4;  // a warp's staged prefixes (+ the end), 16-byte multiple
+// Words of the CTA's uint32 shared buffer: scan scratch, the heavy queue, then
+// one staging area per warp (16-byte aligned).
+template <int THREADS>
+constexpr int shj_words()
+{
+    return ((THREADS + 35 + kBigParents + 3) / 4) * 4 + (THREADS / 32) * kWs;
+}
+template <int THREADS>
+constexpr int ws_offset()
+{
+    return ((THREADS + 35 + kBigParents + 3) / 4) * 4;
+}
 
 // Eight consecutive elements starting at a 32-byte aligned address (float,
 // uint32) or a 64-byte aligned one (double) with vector loads and stores.
@@ -659,81 +676,75 @@ struct FilterRun {
         }
         __syncthreads();
         n_empty = ecarry;
-        // parent p fills the empty slots ep[sS_p, sS_{p+1}) with copies of
-        // itself (empty slot k takes the last parent with sS <= k); parents
-        // with more than 32 copies are queued and copied by the whole CTA
+        // Placement: empty slot ep[k] takes a copy of the parent p with
+        // sS_p <= k < sS_{p+1} (the k-th surplus copy goes to the k-th empty
+        // slot).  Per tile a warp stages the prefixes of its 256 parents in
+        // shared memory; its lanes then take the warp's empties 32 at a time
+        // (coalesced loads of ep), each finding its parent by a binary search
+        // over the staged prefixes.  Parents are occupied slots and never
+        // written, so loads and stores need no ordering.  A warp with more
+        // than kWarpCopies copies in a tile is queued and copied by the CTA.
         {
-            uint32_t *nbig = shj + THREADS + 34;  // queue length, then queued parents
+            uint32_t *nbig = shj + THREADS + 34;  // queue length, then queued parent groups
             uint32_t *big = nbig + 1;
+            const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            uint32_t *wsw = shj + ws_offset<THREADS>() + warp * kWs;
             if (threadIdx.x == 0) *nbig = 0;
             __syncthreads();
             const uint32_t ne = ecarry;
-            // V consecutive parents per thread; their prefixes and particles
-            // are loaded before any copy is stored
-            for (uint32_t q0 = threadIdx.x * V; q0 < N32; q0 += TILE) {
-                uint32_t ss[V + 1];
-                R xv[V];
-                double xsv[V];
+            for (uint32_t b = 0; b < N32; b += TILE) {
+                const uint32_t P0 = b + warp * kWarpParents;
+                if (P0 >= N32) continue;  // warp-uniform; the loop holds no CTA barrier
+                const uint32_t q0 = P0 + lane * V;
+                uint32_t ss[V];
                 if (q0 + V <= N32) {
-                    uint32_t s8[V];
-                    ld8(sS + q0, s8);
-#pragma unroll
-                    for (int k = 0; k < V; ++k) ss[k] = s8[k];
-                    ss[V] = q0 + V < N32 ? sS[q0 + V] : ne;
-                    ld8(xc + q0, xv);
-                    if constexpr (SHADOW) ld8(xsc + q0, xsv);
+                    ld8(sS + q0, ss);
                 } else {
 #pragma unroll
-                    for (int k = 0; k <= V; ++k) ss[k] = q0 + k < N32 ? sS[q0 + k] : ne;
-#pragma unroll
-                    for (int k = 0; k < V; ++k) {
-                        xv[k] = q0 + k < N32 ? xc[q0 + k] : R(0);
-                        if constexpr (SHADOW) xsv[k] = q0 + k < N32 ? xsc[q0 + k] : 0.0;
+                    for (int k = 0; k < V; ++k) ss[k] = q0 + k < N32 ? sS[q0 + k] : ne;
+                }
+                st8(wsw + lane * V, ss);
+                if (lane == 31) wsw[kWarpParents] = q0 + V < N32 ? sS[q0 + V] : ne;
+                __syncwarp();
+                const uint32_t A = wsw[0], B = wsw[kWarpParents];
+                uint32_t queued = 0;
+                if (B - A > kWarpCopies && lane == 0) {
+                    const uint32_t q = atomicAdd(nbig, 1u);
+                    if (q < kBigParents) {
+                        big[q] = P0;
+                        queued = 1;
                     }
                 }
-                // the group's copies are the empties ep[ss[0], ss[V]), parent
-                // k owning [ss[k], ss[k+1]); heavy parents go to the queue
-                uint32_t heavy = 0;
+                queued = __shfl_sync(0xffffffffu, queued, 0);
+                if (!queued) {
+                    for (uint32_t e = A + lane; e < B; e += 32) {
+                        uint32_t lo = 0;
 #pragma unroll
-                for (int k = 0; k < V; ++k) {
-                    if (q0 + k < N32 && ss[k + 1] - ss[k] > 32) {
-                        const uint32_t q = atomicAdd(nbig, 1u);
-                        if (q < kBigParents) {
-                            big[q] = q0 + k;
-                            heavy |= 1u << k;
-                        }
+                        for (uint32_t h = kWarpParents / 2; h >= 1; h >>= 1) lo += wsw[lo + h] <= e ? h : 0;
+                        const uint32_t slot = ep[e];
+                        xc[slot] = xc[P0 + lo];
+                        if constexpr (SHADOW) xsc[slot] = xsc[P0 + lo];
                     }
                 }
-                // eight empties at a time: their slots are loaded together,
-                // then each takes its parent's particle
-                for (uint32_t cb = ss[0]; cb < ss[V]; cb += 8) {
-                    uint32_t e[8];
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) e[i] = cb + i < ss[V] ? ep[cb + i] : 0u;
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        const uint32_t c = cb + i;
-                        if (c >= ss[V]) break;
-                        int k = 0;
-#pragma unroll
-                        for (int q = 1; q < V; ++q) k += ss[q] <= c ? 1 : 0;
-                        if (heavy & (1u << k)) continue;
-                        xc[e[i]] = xv[k];
-                        if constexpr (SHADOW) xsc[e[i]] = xsv[k];
-                    }
-                }
+                __syncwarp();  // the staging area is rewritten by the next tile
             }
             __syncthreads();
             const uint32_t nb = min(*nbig, kBigParents);
+            uint32_t *wsc = shj + ws_offset<THREADS>();  // warp 0's area, now free
             for (uint32_t i = 0; i < nb; ++i) {
-                const uint32_t p = big[i];
-                const uint32_t s0 = sS[p], s1 = p + 1 < N32 ? sS[p + 1] : ne;
-                const R v = xc[p];
-                for (uint32_t k = s0 + threadIdx.x; k < s1; k += THREADS) {
-                    const uint32_t e = ep[k];
-                    xc[e] = v;
-                    if constexpr (SHADOW) xsc[e] = xsc[p];
+                const uint32_t P0 = big[i];
+                for (uint32_t k = threadIdx.x; k <= kWarpParents; k += THREADS) wsc[k] = P0 + k < N32 ? sS[P0 + k] : ne;
+                __syncthreads();
+                const uint32_t A = wsc[0], B = wsc[kWarpParents];
+                for (uint32_t e = A + threadIdx.x; e < B; e += THREADS) {
+                    uint32_t lo = 0;
+#pragma unroll
+                    for (uint32_t h = kWarpParents / 2; h >= 1; h >>= 1) lo += wsc[lo + h] <= e ? h : 0;
+                    const uint32_t slot = ep[e];
+                    xc[slot] = xc[P0 + lo];
+                    if constexpr (SHADOW) xsc[slot] = xsc[P0 + lo];
                 }
+                __syncthreads();
             }
         }
         __syncthreads();
@@ -754,7 +765,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_pf_batched(const BatchedFilte
     __shared__ double shd[33];
     __shared__ R shr[33];
     __shared__ unsigned long long shu[33];
-    __shared__ uint32_t shj[THREADS + 35 + kBigParents];
+    __shared__ __align__(16) uint32_t shj[shj_words<THREADS>()];
     __shared__ int sh_f;
     while (true) {
         if (threadIdx.x == 0) {
@@ -824,7 +835,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_adjoint(const BatchedFilter *
 {
     __shared__ double shd[33];
     __shared__ unsigned long long shu[33];
-    __shared__ uint32_t shj[THREADS + 35 + kBigParents];
+    __shared__ __align__(16) uint32_t shj[shj_words<THREADS>()];
     __shared__ int sh_f;
     const int C = A.C;
     const uint64_t slot = blockIdx.x, cn = static_cast<uint64_t>(C) * A.nmax;
