@@ -59,6 +59,23 @@ __device__ __forceinline__ T block_inclusive_sum(T v, T *sh, T *total)
     return inc;
 }
 
+// Inclusive prefix sum over the CTA with a single barrier: every warp scans
+// the warp totals itself.  `sh` needs 32 elements; the caller must separate
+// two uses of the same `sh` by another CTA barrier (no trailing barrier here).
+template <typename T>
+__device__ __forceinline__ T block_inclusive_sum_1b(T v, T *sh, T *total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const T inc = warp_inclusive_sum(v);
+    if (lane == 31) sh[warp] = inc;
+    __syncthreads();
+    T w = lane < nw ? sh[lane] : T(0);
+    w = warp_inclusive_sum(w);
+    const T before = __shfl_sync(0xffffffffu, w, warp > 0 ? warp - 1 : 0);
+    *total = __shfl_sync(0xffffffffu, w, nw - 1);
+    return warp > 0 ? before + inc : inc;
+}
+
 template <typename T>
 __device__ __forceinline__ T block_sum(T v, T *sh)
 {

@@ -594,9 +594,30 @@ struct FilterRun {
         constexpr uint32_t TILE = THREADS * V;
         const uint64_t U64 = U < 1.0 ? static_cast<uint64_t>(U * 0x1p64) : ~0ull;
         const uint32_t N32 = static_cast<uint32_t>(N);
+        // RN(e RN(1/S)) 2^62 == RN(e (RN(1/S) 2^62)): a power-of-two scale
+        // commutes with rounding (e RN(1/S) >= 2^-181 when nonzero, far from
+        // the subnormals)
+        const double invS62 = invS * 0x1p62;
+        // grid points (U + i) / N, i < N, at or below c 2^-62, for the
+        // cumulative weight c (exact 128-bit arithmetic)
+        auto count = [N32, U64](uint64_t c) -> uint32_t {
+            // X = 4 N c as a 128-bit number (hi, lo)
+            const uint64_t lo = static_cast<uint64_t>(N32) * c, hi = __umul64hi(static_cast<uint64_t>(N32), c);
+            const uint64_t xhi = (hi << 2) | (lo >> 62), xlo = lo << 2;
+            if (xhi == 0 && xlo <= U64) return 0;
+            // floor((X - U64 - 1) / 2^64) + 1: the high word of X - (U64 + 1),
+            // plus one
+            const uint64_t borrow = (U64 == ~0ull || xlo < U64 + 1) ? 1 : 0;
+            const uint64_t dhi = xhi - borrow;
+            return dhi + 1 > N32 ? N32 : static_cast<uint32_t>(dhi + 1);
+        };
+        // Two CTA barriers per tile: one per scan.  The scans use different
+        // scratch (shu, shj + THREADS + 1), so each scratch's next writer is
+        // behind the other scan's barrier.
         unsigned long long *shw64 = shu;
+        uint32_t *she = shj + THREADS + 1;
         uint64_t carry = 0;
-        uint32_t jprev = 0, ecarry = 0;
+        uint32_t ecarry = 0;
         for (uint32_t b = 0; b < N32; b += TILE) {
             const uint32_t q0 = b + threadIdx.x * V;
             const bool whole = q0 + V <= N32;  // all V particles exist
@@ -611,49 +632,31 @@ struct FilterRun {
             unsigned long long acc = 0;
 #pragma unroll
             for (int k = 0; k < V; ++k) {
-                const double w = (whole || q0 + k < N32) ? static_cast<double>(Math<R>::exp(Math<R>::sub(lv[k], M))) * invS : 0.0;
-                acc += __double2ull_rn(w * 0x1p62);
+                const double w62 = (whole || q0 + k < N32)
+                    ? static_cast<double>(Math<R>::exp(Math<R>::sub(lv[k], M))) * invS62 : 0.0;
+                acc += __double2ull_rn(w62);
                 C[k] = acc;
             }
             unsigned long long tot;
-            const uint64_t excl = block_inclusive_sum(acc, shw64, &tot) - acc;
-            const uint64_t base = carry + excl;
+            const uint64_t base = carry + block_inclusive_sum_1b(acc, shw64, &tot) - acc;
             carry += tot;
+            // j of the particle before q0: its cumulative weight is base
+            // (j_{-1} = 0 from base = 0)
+            const uint32_t jm = count(base);
             uint32_t j[V];
 #pragma unroll
             for (int k = 0; k < V; ++k) {
                 const uint32_t p = q0 + k;
-                const uint64_t c = base + C[k];
-                // X = 4 N c as a 128-bit number (hi, lo)
-                const uint64_t lo = static_cast<uint64_t>(N32) * c, hi = __umul64hi(static_cast<uint64_t>(N32), c);
-                const uint64_t xhi = (hi << 2) | (lo >> 62), xlo = lo << 2;
-                uint32_t cnt;
-                if (xhi == 0 && xlo <= U64) {
-                    cnt = 0;
-                } else {
-                    // floor((X - U64 - 1) / 2^64) + 1: the high word of
-                    // X - (U64 + 1), plus one
-                    const uint64_t borrow = (U64 == ~0ull || xlo < U64 + 1) ? 1 : 0;
-                    const uint64_t dhi = xhi - borrow;
-                    cnt = dhi + 1 > N32 ? N32 : static_cast<uint32_t>(dhi + 1);
-                }
-                j[k] = (p + 1 >= N32) ? N32 : cnt;
+                j[k] = (p + 1 >= N32) ? N32 : count(base + C[k]);
             }
-            shj[threadIdx.x + 1] = j[V - 1];
-            if (threadIdx.x == 0) shj[0] = jprev;
-            __syncthreads();
-            uint32_t jm = shj[threadIdx.x];
-            jprev = shj[THREADS];
             uint32_t ne = 0;
 #pragma unroll
             for (int k = 0; k < V; ++k) {
                 const uint32_t p = q0 + k;
-                const uint32_t jk = j[k];
-                ne += (p < N32 && jk == (k == 0 ? jm : j[k - 1])) ? 1u : 0u;
+                ne += (p < N32 && j[k] == (k == 0 ? jm : j[k - 1])) ? 1u : 0u;
             }
             uint32_t etot;
-            const uint32_t eex = block_inclusive_sum(ne, shj + THREADS + 1, &etot) - ne;
-            uint32_t E = ecarry + eex;
+            uint32_t E = ecarry + block_inclusive_sum_1b(ne, she, &etot) - ne;
             ecarry += etot;
             uint32_t sv[V];
 #pragma unroll
