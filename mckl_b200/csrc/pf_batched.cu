@@ -599,17 +599,19 @@ struct FilterRun {
         // the subnormals)
         const double invS62 = invS * 0x1p62;
         // grid points (U + i) / N, i < N, at or below c 2^-62, for the
-        // cumulative weight c (exact 128-bit arithmetic)
-        auto count = [N32, U64](uint64_t c) -> uint32_t {
-            // X = 4 N c as a 128-bit number (hi, lo)
-            const uint64_t lo = static_cast<uint64_t>(N32) * c, hi = __umul64hi(static_cast<uint64_t>(N32), c);
-            const uint64_t xhi = (hi << 2) | (lo >> 62), xlo = lo << 2;
-            if (xhi == 0 && xlo <= U64) return 0;
-            // floor((X - U64 - 1) / 2^64) + 1: the high word of X - (U64 + 1),
-            // plus one
-            const uint64_t borrow = (U64 == ~0ull || xlo < U64 + 1) ? 1 : 0;
-            const uint64_t dhi = xhi - borrow;
-            return dhi + 1 > N32 ? N32 : static_cast<uint32_t>(dhi + 1);
+        // cumulative weight c: j = clamp(ceil((X - U64) / 2^64), 0, N) with
+        // X = 4 N c, exact and branch-free.  With D = X - (U64 + 1) as a
+        // 128-bit difference, j = 0 when D < 0, else (D >> 64) + 1.  N c is
+        // formed from two 32 x 32 -> 64-bit products (c < 2^63).
+        const uint64_t ulo = U64 + 1;  // U64 + 1 = (uhi, ulo); wraps when U64 = 2^64 - 1
+        const int64_t uhi = U64 == ~0ull ? 1 : 0;
+        auto count = [N32, ulo, uhi](uint64_t c) -> uint32_t {
+            const uint64_t a = static_cast<uint64_t>(N32) * static_cast<uint32_t>(c);
+            const uint64_t m = static_cast<uint64_t>(N32) * static_cast<uint32_t>(c >> 32) + (a >> 32);
+            // N c = m 2^32 + (a mod 2^32); X = 4 N c = (m >> 30) 2^64 + xlo
+            const uint64_t xlo = ((m << 32) | static_cast<uint32_t>(a)) << 2;
+            const int64_t dhi = static_cast<int64_t>(m >> 30) - uhi - (xlo < ulo ? 1 : 0);
+            return dhi < 0 ? 0u : (dhi + 1 >= static_cast<int64_t>(N32) ? N32 : static_cast<uint32_t>(dhi) + 1u);
         };
         // Two CTA barriers per tile: one per scan.  The scans use different
         // scratch (shu, shj + THREADS + 1), so each scratch's next writer is
