@@ -213,7 +213,7 @@ def bench_smc(args, rank, world, dev):
     T = args.obs
     w = mb.batched_workload(F=args.filters, T=T, seed=1234 + 7919 * rank)
     ps_per_step = float(w["N"].sum()) * T
-    b = make_filters(mb, w)
+    b = make_filters(mb, w, threshold=args.threshold)
     if args.shape:
         th, cps = (int(v) for v in args.shape.split("x"))
         b.config(th, cps)
@@ -268,7 +268,7 @@ def bench_smc(args, rank, world, dev):
     if rank == 0:
         import oracle as O
 
-        bs = make_filters(mb, w, shadow=True)
+        bs = make_filters(mb, w, shadow=True, threshold=args.threshold)
         best = min(trials, key=lambda r: r[2])
         bs.config(best[0], best[1])
         bs.run()
@@ -698,10 +698,13 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mckl_b200", choices=["mckl_b200", "reference"])
-    ap.add_argument("--workload", default="smc", choices=["smc", "rng"])
+    ap.add_argument("--workload", default="smc", choices=["smc", "rng", "callers"],
+                    help="callers: only the index matrix / weighted estimate / PMCMC measurements, one JSON object")
     ap.add_argument("--filters", type=int, default=4096)
     ap.add_argument("--obs", type=int, default=500)
     ap.add_argument("--parts", default="all", choices=["all", "timed"])
+    ap.add_argument("--threshold", type=float, default=0.5,
+                    help="resample when ESS < threshold N (0: never, above 1: every step)")
     ap.add_argument("--shape", default="", help="threads x CTAs per SM (e.g. 512x2) instead of the autotuner")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -710,7 +713,7 @@ def main():
     smc = args.workload == "smc"
     if smc:
         cfg = {"workload": f"batched SMC: {args.filters} AR(1) bootstrap filters, N log-uniform in [256, 65536], "
-                           f"T = {args.obs}, systematic resampling at ESS < N/2, FP32 propagation + FP64 "
+                           f"T = {args.obs}, systematic resampling at ESS < {args.threshold:g} N, FP32 propagation + FP64 "
                            "normaliser/scan/logL, one persistent launch replayed from a CUDA graph",
                "filters": args.filters, "T": args.obs,
                "parallelism": f"{world} rank(s), {args.filters} filters each (own seeds)",
@@ -725,6 +728,9 @@ def main():
 
     if args.impl == "reference":
         if rank != 0:
+            return
+        if args.workload == "callers":
+            print(json.dumps({"impl": "reference", "workload": "callers", "cpu_reference": cpu_callers_reference()}))
             return
         if smc:
             import mckl_b200 as mb  # generates the workload's parameters and observations only
@@ -756,6 +762,16 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     hbm_peak, sm_max, peak_kind = measured_peaks()
+    if args.workload == "callers":
+        if rank == 0:
+            out = {"workload": "callers", "n_gpus": 1, "callers": bench_callers(dev, hbm_peak, peak_kind)}
+            cc = cpu_callers_reference()
+            if cc:
+                out["callers"]["cpu_reference"] = cc
+            print(json.dumps(out))
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
     if smc:
         res = bench_smc(args, rank, world, dev)
         sm_mhz = (res["clocks"] or {}).get("sm_mhz") or sm_max
