@@ -22,7 +22,8 @@ namespace mckl_b200 {
 namespace {
 
 constexpr int kEstThreads = 256;
-constexpr uint64_t kEstChunk = 8192;      // particles per CTA (column-major, narrow row-major)
+constexpr uint64_t kEstChunk = 8192;      // particles per CTA (column-major)
+constexpr uint64_t kEstChunkNarrow = 2048;  // particles per CTA (row-major, d <= 256): several waves of CTAs
 constexpr uint64_t kEstChunkWide = 1024;  // particles per CTA (row-major, d > 256)
 
 // column j = blockIdx.x: the CTAs of one chunk run next to each other and
@@ -48,10 +49,11 @@ __global__ void __launch_bounds__(kEstThreads) k_est_rows_narrow(uint64_t n, uin
     __shared__ double sh[kEstThreads];
     const uint32_t q = kEstThreads / d;  // rows per pass
     const uint32_t t = threadIdx.x;
-    const uint64_t b0 = blockIdx.x * kEstChunk, b1 = min(n, b0 + kEstChunk);
+    const uint64_t b0 = blockIdx.x * kEstChunkNarrow, b1 = min(n, b0 + kEstChunkNarrow);
     double acc = 0.0;
     if (t < q * d) {
         const uint32_t j = t % d;
+#pragma unroll 4
         for (uint64_t i = b0 + t / d; i < b1; i += q) acc = fma(w[i], u[i * d + j], acc);
     }
     sh[t] = acc;
@@ -105,7 +107,7 @@ extern "C" int mckl_b200_weighted_estimate(size_t n, size_t d, int col_major, co
         return MCKL_B200_OK;
     }
     const bool wide = !col_major && d > static_cast<size_t>(kEstThreads);
-    const uint64_t chunk = wide ? kEstChunkWide : kEstChunk;
+    const uint64_t chunk = col_major ? kEstChunk : (wide ? kEstChunkWide : kEstChunkNarrow);
     const uint64_t nb = (n + chunk - 1) / chunk;
     MB_CHECK_ARG(nb <= 0x7fffffffull, "too many particles");
     double *partial = static_cast<double *>(scratch(8, align256(nb * d * sizeof(double)), s));
