@@ -146,16 +146,6 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def max_over_ranks(v, world, dev):
-    if world == 1:
-        return v
-    import torch
-
-    t = torch.tensor([v], device=dev, dtype=torch.float64)
-    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    return float(t.item())
-
-
 def barrier(world):
     if world > 1:
         import torch
@@ -210,8 +200,11 @@ def bench_smc(args, rank, world, dev):
 
     import mckl_b200 as mb
 
+    from mckl_b200.shard import filter_range, job_rate
+
     T = args.obs
-    w = mb.batched_workload(F=args.filters, T=T, seed=1234 + 7919 * rank)
+    first, _ = filter_range(rank, args.filters)
+    w = mb.batched_workload(F=args.filters, T=T, seed=1234, first=first)
     ps_per_step = float(w["N"].sum()) * T
     b = make_filters(mb, w, threshold=args.threshold)
     if args.shape:
@@ -236,8 +229,7 @@ def bench_smc(args, rank, world, dev):
     torch.cuda.synchronize()
     launches = mb.launch_count() - l0
     clk = clocks.stop()
-    elapsed = max_over_ranks(t0.elapsed_time(t1) / 1e3, world, dev)
-    value = world * ps_per_step * args.steps / elapsed
+    value, elapsed = job_rate(ps_per_step * args.steps, t0.elapsed_time(t1) / 1e3, world, dev)
     ll, nres = b.results()
     out = dict(value=value, elapsed=elapsed, launches=launches, clocks=clk, ps_per_step=ps_per_step, w=w, ll=ll)
     if args.parts == "timed":
@@ -259,9 +251,9 @@ def bench_smc(args, rank, world, dev):
         b.results()
     h1.record(stream)
     torch.cuda.synchronize()
-    e2e_elapsed = max_over_ranks(h0.elapsed_time(h1) / 1e3, world, dev)
+    e2e_value, _ = job_rate(ps_per_step * e2e_steps, h0.elapsed_time(h1) / 1e3, world, dev)
     b.close()
-    out["e2e"] = {"value": world * ps_per_step * e2e_steps / e2e_elapsed, "unit": "particle-steps/s",
+    out["e2e"] = {"value": e2e_value, "unit": "particle-steps/s",
                   "h2d_bytes_per_step": int(w["y"].nbytes), "d2h_bytes_per_step": int(len(w["N"]) * 12)}
     extra = {"autotune": [{"threads": t, "ctas_per_sm": c, "ms": round(m, 3)} for (t, c, m) in trials],
              "resampling_events_per_step": int(nres.sum())}
@@ -519,9 +511,11 @@ def bench_rng(rank, world, dev, steps, warmup, e2e=True, clocks_on=True):
     buf32 = torch.empty(n, dtype=torch.int32, device=dev)
     buf64 = torch.empty(n, dtype=torch.float64, device=dev)
 
+    from mckl_b200.shard import job_rate, rng_counter
+
     def fresh(eng):
         g = mb.ENGINES[eng](42)
-        g.ctr = (0, rank)  # rank-private counter range
+        g.ctr = rng_counter(rank)  # rank-private counter range
         return g
 
     stream = torch.cuda.current_stream()
@@ -553,9 +547,9 @@ def bench_rng(rank, world, dev, steps, warmup, e2e=True, clocks_on=True):
     torch.cuda.synchronize()
     launches = mb.launch_count() - launches0
     clk = clocks.stop() if clocks else None
-    elapsed = max_over_ranks(t0.elapsed_time(t1) / 1e3, world, dev)
     bytes_per_step = sum(n * bpv for (_, _, _, bpv) in ops)
-    value = world * bytes_per_step * steps / elapsed / 1e9
+    rate, elapsed = job_rate(bytes_per_step * steps, t0.elapsed_time(t1) / 1e3, world, dev)
+    value = rate / 1e9
     per_op = {}
     for (name, e0, e1, nbytes) in rec:
         d = per_op.setdefault(name, {"ms": 0.0, "bytes": nbytes, "calls": 0})
@@ -609,8 +603,8 @@ def bench_rng(rank, world, dev, steps, warmup, e2e=True, clocks_on=True):
             run_op(mb, call, fresh(eng), n, hbuf32, hbuf64)
         h1.record(stream)
         torch.cuda.synchronize()
-        e2e_elapsed = max_over_ranks(h0.elapsed_time(h1) / 1e3, world, dev)
-        out["e2e"] = {"value": world * bytes_per_step / e2e_elapsed / 1e9, "unit": "GB/s",
+        e2e_rate, _ = job_rate(bytes_per_step, h0.elapsed_time(h1) / 1e3, world, dev)
+        out["e2e"] = {"value": e2e_rate / 1e9, "unit": "GB/s",
                       "h2d_bytes_per_step": 0, "d2h_bytes_per_step": bytes_per_step,
                       "note": "kernels write page-locked host buffers directly"}
     return out

@@ -295,17 +295,19 @@ class BatchedFilters:
             pass
 
 
-def batched_workload(F=4096, T=500, seed=1234, nmin=256, nmax=65536):
-    """The batched configuration: filter parameters from Philox4x32(seed)
-    canonical uniforms (phi ~ U[0.5, 0.99], sx ~ U[0.5, 2], sy ~ U[0.2, 1],
+def batched_workload(F=4096, T=500, seed=1234, nmin=256, nmax=65536, first=0):
+    """The batched configuration, filters first .. first + F - 1 of it: filter
+    parameters from Philox4x32(seed) canonical uniforms, four per filter in
+    filter order (phi ~ U[0.5, 0.99], sx ~ U[0.5, 2], sy ~ U[0.2, 1],
     N = round(exp(U[ln nmin, ln nmax]))), observations of filter f simulated
     with Philox4x32(key f, 10) (2T + 2 standard normals: x_0 = sd0 z_0,
     x_t = phi x_{t-1} + sx z_t, y_t = x_t + sy z_{T+t}); model keys (f, 11),
-    resampling keys (f, 12)."""
+    resampling keys (f, 12).  A rank of a multi-GPU run takes its own range
+    of filters (mckl_b200.shard.filter_range)."""
     torch = _torch()
     g = Philox4x32()
     g.key = (seed, 0)
-    u = u01_canonical_distribution(g, 4 * F, dtype="f64").cpu().numpy().reshape(F, 4)
+    u = u01_canonical_distribution(g, 4 * (first + F), dtype="f64").cpu().numpy().reshape(first + F, 4)[first:]
     phi = 0.5 + 0.49 * u[:, 0]
     sx = 0.5 + 1.5 * u[:, 1]
     sy = 0.2 + 0.8 * u[:, 2]
@@ -313,7 +315,7 @@ def batched_workload(F=4096, T=500, seed=1234, nmin=256, nmax=65536):
     z = torch.empty((F, 2 * T + 2), dtype=torch.float64, device="cuda")
     for f in range(F):
         gf = Philox4x32()
-        gf.key = (f, 10)
+        gf.key = (first + f, 10)
         normal_distribution(gf, 2 * T + 2, z[f])
     z = z.cpu().numpy()
     sd0 = sx / np.sqrt(1 - phi * phi)
@@ -322,8 +324,9 @@ def batched_workload(F=4096, T=500, seed=1234, nmin=256, nmax=65536):
     for t in range(1, T + 1):
         x = phi * x + sx * z[:, t]
         y[:, t] = x + sy * z[:, T + t]
-    mkeys = np.stack([np.arange(F), np.full(F, 11)], axis=1).astype(np.uint32)
-    rkeys = np.stack([np.arange(F), np.full(F, 12)], axis=1).astype(np.uint32)
+    ids = np.arange(first, first + F)
+    mkeys = np.stack([ids, np.full(F, 11)], axis=1).astype(np.uint32)
+    rkeys = np.stack([ids, np.full(F, 12)], axis=1).astype(np.uint32)
     return dict(N=N, y=y, phi=phi, sx=sx, sy=sy, sd0=sd0, mkeys=mkeys, rkeys=rkeys)
 
 
