@@ -10,6 +10,7 @@
 // particles as written; for row-major output a CTA stages a few iterations of
 // its particles' lines in shared memory and writes whole row segments.
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -116,6 +117,32 @@ __global__ void __launch_bounds__(256) k_index_matrix_rows(uint64_t N, uint64_t 
     }
 }
 
+// Page-locked staging for the upload (vector addresses, sizes, error word)
+// and the error read-back: small copies from pageable memory go through the
+// driver's staging buffers and cost several microseconds each.  One buffer
+// per process, grown on demand, held for the whole call.
+std::mutex g_stage_mu;
+uint64_t *g_stage = nullptr;
+size_t g_stage_words = 0;
+
+uint64_t *stage_words(size_t words)
+{
+    if (words > g_stage_words) {
+        if (g_stage) cudaFreeHost(g_stage);
+        g_stage = nullptr;
+        g_stage_words = 0;
+        const size_t want = std::max<size_t>(words, 4096);
+        if (cudaHostAlloc(reinterpret_cast<void **>(&g_stage), want * sizeof(uint64_t), cudaHostAllocPortable) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            g_stage = nullptr;
+            return nullptr;
+        }
+        g_stage_words = want;
+    }
+    return g_stage;
+}
+
 }  // namespace
 
 }  // namespace mckl_b200
@@ -137,13 +164,21 @@ extern "C" int mckl_b200_index_matrix(size_t N, size_t R, const uint64_t *const 
     auto **dptr = reinterpret_cast<const uint64_t **>(scr);
     auto *dsz = reinterpret_cast<uint64_t *>(scr + R * sizeof(uint64_t));
     auto *derr = reinterpret_cast<uint32_t *>(scr + 2 * R * sizeof(uint64_t));
-    std::vector<uint64_t> up(words, 0);
     for (size_t r = 0; r < R; ++r) {
         MB_CHECK_ARG(index_host[r] != nullptr || sizes_host[r] == 0, "null index vector");
+    }
+    std::lock_guard<std::mutex> lock(g_stage_mu);  // the staging buffer is reused once this call has synchronized
+    uint64_t *up = stage_words(words + 1);
+    if (!up) {
+        set_error("mckl_b200_index_matrix: page-locked staging buffer allocation failed");
+        return MCKL_B200_ERR_NOMEM;
+    }
+    for (size_t r = 0; r < R; ++r) {
         up[r] = reinterpret_cast<uint64_t>(index_host[r]);
         up[R + r] = sizes_host[r];
     }
-    MB_CUDA(cudaMemcpyAsync(scr, up.data(), words * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+    up[2 * R] = 0;
+    MB_CUDA(cudaMemcpyAsync(scr, up, words * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -161,10 +196,11 @@ extern "C" int mckl_b200_index_matrix(size_t N, size_t R, const uint64_t *const 
         k_index_matrix_rows<<<static_cast<unsigned>(blocks), 256, 0, s>>>(N, R, dptr, dsz, out, derr);
     }
     MB_LAUNCH_CHECK();
-    uint32_t herr = 0;
-    MB_CUDA(cudaMemcpyAsync(&herr, derr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    uint32_t *herr_p = reinterpret_cast<uint32_t *>(up + words);
+    *herr_p = 0;
+    MB_CUDA(cudaMemcpyAsync(herr_p, derr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     MB_CUDA(cudaStreamSynchronize(s));
-    if (herr) {
+    if (*herr_p) {
         set_error("mckl_b200_index_matrix: a parent index is outside the previous iteration's particles");
         return MCKL_B200_ERR_ARG;
     }
