@@ -77,6 +77,76 @@ struct PhiloxGen {
     }
 };
 
+__host__ __device__ inline uint32_t mulhi32(uint32_t a, uint32_t b)
+{
+#ifdef __CUDA_ARCH__
+    return __umulhi(a, b);
+#else
+    return static_cast<uint32_t>((static_cast<uint64_t>(a) * b) >> 32);
+#endif
+}
+
+// Philox blocks of one launch whose counters differ only in the low 32-bit
+// word s0 (s1, s2, s3 fixed): in the first round the product of s2 does not
+// depend on the block, so neither do the first round's outputs s0' and s1',
+// nor the second round's product of s0'.  Those are folded once per launch
+// (make); a block then takes 36 of the 40 multiply halves.  The output is
+// the same as PhiloxGen::block on the full counter.
+struct PhiloxLo {
+    uint32_t lo;            // s0 of block 0 of the launch
+    uint32_t k1s3;          // k1 ^ s3 (first round, third word)
+    uint32_t ca, cb, lo0c;  // second round: (k0 + W0) ^ s1', (k1 + W1) ^ hi(s0' M0), lo(s0' M0)
+    uint32_t a2, b2;        // keys of the third round
+
+    __host__ __device__ static PhiloxLo make(const PhiloxGen &g, const Ctr &base)
+    {
+        const uint32_t s1 = static_cast<uint32_t>(base.w[0] >> 32);
+        const uint32_t s2 = static_cast<uint32_t>(base.w[1]);
+        const uint32_t s3 = static_cast<uint32_t>(base.w[1] >> 32);
+        const uint32_t s0p = g.k0 ^ s1 ^ mulhi32(s2, 0xCD9E8D57u);
+        const uint32_t s1p = s2 * 0xCD9E8D57u;
+        PhiloxLo p;
+        p.lo = static_cast<uint32_t>(base.w[0]);
+        p.k1s3 = g.k1 ^ s3;
+        p.ca = (g.k0 + 0x9E3779B9u) ^ s1p;
+        p.cb = (g.k1 + 0xBB67AE85u) ^ mulhi32(s0p, 0xD2511F53u);
+        p.lo0c = s0p * 0xD2511F53u;
+        p.a2 = g.k0 + 2u * 0x9E3779B9u;
+        p.b2 = g.k1 + 2u * 0xBB67AE85u;
+        return p;
+    }
+
+    // block i of the launch (counter low word lo + i, no carry into s1)
+    __host__ __device__ __forceinline__ void block(uint32_t i, uint32_t out[4]) const
+    {
+        const uint32_t s0 = lo + i;
+        const uint32_t t2 = k1s3 ^ mulhi32(s0, 0xD2511F53u);  // first round
+        const uint32_t t3 = s0 * 0xD2511F53u;
+        uint32_t x0 = ca ^ mulhi32(t2, 0xCD9E8D57u);  // second round
+        uint32_t x1 = t2 * 0xCD9E8D57u;
+        uint32_t x2 = cb ^ t3;
+        uint32_t x3 = lo0c;
+        uint32_t a = a2, b = b2;
+#pragma unroll
+        for (int r = 2; r < 10; ++r) {
+            const uint32_t hi2 = mulhi32(x2, 0xCD9E8D57u);
+            const uint32_t lo2 = x2 * 0xCD9E8D57u;
+            const uint32_t hi0 = mulhi32(x0, 0xD2511F53u);
+            const uint32_t lo0 = x0 * 0xD2511F53u;
+            x0 = a ^ x1 ^ hi2;
+            x1 = lo2;
+            x2 = b ^ x3 ^ hi0;
+            x3 = lo0;
+            a += 0x9E3779B9u;
+            b += 0xBB67AE85u;
+        }
+        out[0] = x0;
+        out[1] = x1;
+        out[2] = x2;
+        out[3] = x3;
+    }
+};
+
 // ---------------------------------------------------------------------------
 // Threefry4x64-20.  The key-injection words of all six injections are
 // precomputed on the host (they do not depend on the counter).

@@ -76,17 +76,23 @@ __global__ void __launch_bounds__(kEstThreads) k_est_rows_wide(uint64_t n, uint6
     partial[j * gridDim.x + blockIdx.x] = acc;
 }
 
-// one warp per column: lane l adds partials l, l + 32, ... in order, then a
-// fixed butterfly
-__global__ void k_est_final(uint64_t d, uint64_t nb, const double *partial, double *result)
+// one CTA per column: thread t adds partials t, t + 256, ... into four
+// accumulators (four loads in flight), then a fixed CTA tree
+__global__ void __launch_bounds__(kEstThreads) k_est_final(uint64_t nb, const double *partial, double *result)
 {
-    const uint64_t j = blockIdx.x * static_cast<uint64_t>(blockDim.x >> 5) + (threadIdx.x >> 5);
-    const unsigned lane = threadIdx.x & 31;
-    if (j >= d) return;
-    double s = 0.0;
-    for (uint64_t b = lane; b < nb; b += 32) s += partial[j * nb + b];
-    s = warp_sum(s);
-    if (lane == 0) result[j] = s;
+    __shared__ double shd[33];
+    const double *pj = partial + static_cast<uint64_t>(blockIdx.x) * nb;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    uint64_t b = threadIdx.x;
+    for (; b + 3 * kEstThreads < nb; b += 4 * kEstThreads) {
+        a0 += pj[b];
+        a1 += pj[b + kEstThreads];
+        a2 += pj[b + 2 * kEstThreads];
+        a3 += pj[b + 3 * kEstThreads];
+    }
+    for (; b < nb; b += kEstThreads) a0 += pj[b];
+    const double s = block_sum((a0 + a1) + (a2 + a3), shd);
+    if (threadIdx.x == 0) result[blockIdx.x] = s;
 }
 
 }  // namespace
@@ -123,7 +129,7 @@ extern "C" int mckl_b200_weighted_estimate(size_t n, size_t d, int col_major, co
         k_est_rows_wide<<<dim3(static_cast<unsigned>(nb), tiles), kEstThreads, 0, s>>>(n, d, u, w, partial);
     }
     MB_LAUNCH_CHECK();
-    k_est_final<<<static_cast<unsigned>((d + 7) / 8), 256, 0, s>>>(d, nb, partial, result);
+    k_est_final<<<static_cast<unsigned>(d), kEstThreads, 0, s>>>(nb, partial, result);
     MB_LAUNCH_CHECK();
     return MCKL_B200_OK;
 }

@@ -205,6 +205,34 @@ __global__ void __launch_bounds__(256) k_blocks(G g, Ctr base, uint64_t nblk, ty
     }
 }
 
+// k_blocks for Philox launches whose block counters differ only in their low
+// word (PhiloxLo: the counter-independent products folded once per launch).
+template <typename W, class F>
+__global__ void __launch_bounds__(256) k_blocks_plo(PhiloxLo p, uint64_t nblk, typename F::out_t *out, F f)
+{
+    using R = typename F::out_t;
+    constexpr int WPB = PhiloxGen::kWords / WordView<W>::kPer32;
+    constexpr int OPB = WPB / F::kIn;
+    constexpr int U = F::kCheap ? 4 : 1;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t b0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; b0 < nblk; b0 += U * stride) {
+#pragma unroll
+        for (int i = 0; i < U; ++i) {
+            const uint64_t b = b0 + i * stride;
+            if (b >= nblk) break;
+            uint32_t blk[PhiloxGen::kWords];
+            p.block(static_cast<uint32_t>(b), blk);
+            W w[WPB];
+#pragma unroll
+            for (int j = 0; j < WPB; ++j) w[j] = WordView<W>::get(blk, j);
+            R o[OPB];
+#pragma unroll
+            for (int j = 0; j < OPB; ++j) o[j] = f(w + j * F::kIn);
+            store_aligned<R, OPB>(out + b * OPB, o);
+        }
+    }
+}
+
 // Staged shape: outputs [0, n) consume stream words off + kIn * [0, n) counted
 // from word 0 of block `base`.  A CTA stages TB blocks per tile.
 template <class G, typename W, class F, int TB>
@@ -349,7 +377,16 @@ static int launch_words(const G &g, const Ctr &B, uint32_t off, uint64_t n, type
     const int ctas = std::is_same<G, ArsGen>::value ? 6 : 8;
     if (aligned) {
         const uint64_t nblk = n / OPB;
-        if (nblk) {
+        bool done_blocks = false;
+        if constexpr (std::is_same<G, PhiloxGen>::value) {
+            // no carry out of the low counter word within this launch
+            if (nblk && (B.w[0] & 0xffffffffull) + (nblk - 1) <= 0xffffffffull) {
+                k_blocks_plo<W, F><<<grid_for(nblk, 256, ctas), 256, 0, s>>>(PhiloxLo::make(g, B), nblk, out, f);
+                MB_LAUNCH_CHECK();
+                done_blocks = true;
+            }
+        }
+        if (nblk && !done_blocks) {
             MB_CUDA(allow_dyn_smem(k_blocks<G, W, F>, G::kDynSmem));
             k_blocks<G, W, F><<<grid_for(nblk, 256, ctas), 256, G::kDynSmem, s>>>(g, B, nblk, out, f);
             MB_LAUNCH_CHECK();
