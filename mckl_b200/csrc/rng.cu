@@ -172,6 +172,38 @@ struct ExpOut {
     }
 };
 
+// Outputs of 32 bytes per block, lane l of a warp holding block bw + l: each
+// lane writing its own 32 bytes makes every 128-bit store instruction cover
+// half of each sector it touches.  Instead instruction k writes chunk 32k + l
+// of the warp's 1 KiB (half l % 2 of block 16k + l / 2, fetched by shuffles),
+// so each store is contiguous across the warp.  Returns false, storing
+// nothing, unless all 32 blocks of the warp exist (then every lane is here).
+template <typename R, int N>
+__device__ __forceinline__ bool store_warp32(R *out, uint64_t b, uint64_t nblk, const R (&v)[N])
+{
+    static_assert(sizeof(R) * N == 32, "32-byte blocks only");
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t bw = b - lane;  // block of lane 0
+    if (bw + 31 >= nblk) return false;
+    const uint4 c0 = reinterpret_cast<const uint4 *>(v)[0], c1 = reinterpret_cast<const uint4 *>(v)[1];
+    uint4 *dst = reinterpret_cast<uint4 *>(out + bw * N);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int src = 16 * k + static_cast<int>(lane >> 1);
+        uint4 a, h;
+        a.x = __shfl_sync(0xffffffffu, c0.x, src);
+        a.y = __shfl_sync(0xffffffffu, c0.y, src);
+        a.z = __shfl_sync(0xffffffffu, c0.z, src);
+        a.w = __shfl_sync(0xffffffffu, c0.w, src);
+        h.x = __shfl_sync(0xffffffffu, c1.x, src);
+        h.y = __shfl_sync(0xffffffffu, c1.y, src);
+        h.z = __shfl_sync(0xffffffffu, c1.z, src);
+        h.w = __shfl_sync(0xffffffffu, c1.w, src);
+        __stcs(dst + 32 * k + lane, (lane & 1) ? h : a);
+    }
+    return true;
+}
+
 // Aligned shape: nblk whole blocks starting at counter `base`; block b feeds
 // outputs [b * OPB, (b + 1) * OPB).  `out` is 16-byte aligned.
 template <class G, typename W, class F>
@@ -200,6 +232,11 @@ __global__ void __launch_bounds__(256) k_blocks(G g, Ctr base, uint64_t nblk, ty
             R o[OPB];
 #pragma unroll
             for (int j = 0; j < OPB; ++j) o[j] = f(w + j * F::kIn);
+            // the shuffles pay only where the store, not the generator or the
+            // transform, is the limit (Philox with a cheap transform)
+            if constexpr (sizeof(R) * OPB == 32 && F::kCheap && std::is_same<G, PhiloxGen>::value) {
+                if (store_warp32<R, OPB>(out, b, nblk, o)) continue;
+            }
             store_aligned<R, OPB>(out + b * OPB, o);
         }
     }
@@ -228,6 +265,9 @@ __global__ void __launch_bounds__(256) k_blocks_plo(PhiloxLo p, uint64_t nblk, t
             R o[OPB];
 #pragma unroll
             for (int j = 0; j < OPB; ++j) o[j] = f(w + j * F::kIn);
+            if constexpr (sizeof(R) * OPB == 32 && F::kCheap) {
+                if (store_warp32<R, OPB>(out, b, nblk, o)) continue;
+            }
             store_aligned<R, OPB>(out + b * OPB, o);
         }
     }
