@@ -280,6 +280,78 @@ __device__ R gamma_scalar(const GammaParam<R> &k, SW &sw, uint64_t &pos)
     return O::mul(k.beta, r);
 }
 
+// One attempt of algorithm T (0), W (1) or E (3) of the scalar fallback from
+// the words at pos, pos + 1 (E: pos only): these algorithms consume a fixed
+// number of words per attempt (kAttemptWords), so attempt j of the fallback
+// reads words pos0 + kAttemptWords j whatever the earlier attempts did.
+// Returns whether the attempt is accepted; *out = beta r.  The same
+// arithmetic as gamma_scalar's loop bodies.
+template <int ALG>
+struct GammaAttemptWords {
+    static constexpr int value = ALG == 3 ? 1 : 2;
+};
+
+template <typename R, int ALG, class SW>
+__device__ bool gamma_attempt(const GammaParam<R> &k, SW &sw, uint64_t pos, R *out)
+{
+    using O = GOps<R>;
+    const R d = k.d, c = k.c;
+    R r;
+    bool acc;
+    if constexpr (ALG == 0) {
+        R u = O::sub(static_cast<R>(1), RealOps<R>::u01(kOO, sw.at(pos)));
+        R e = -O::log(RealOps<R>::u01(kOO, sw.at(pos + 1)));
+        if (u > d) {
+            u = -O::log(O::mul(c, O::sub(static_cast<R>(1), u)));
+            e = O::add(e, u);
+            u = O::add(d, O::mul(k.alpha, u));
+        }
+        r = O::exp(O::mul(c, O::log(u)));
+        acc = fabs(r) < e;
+    } else if constexpr (ALG == 1) {
+        const R u = -O::log(RealOps<R>::u01(kOO, sw.at(pos)));
+        const R e = -O::log(RealOps<R>::u01(kOO, sw.at(pos + 1)));
+        r = O::exp(O::mul(c, O::log(u)));
+        acc = !(O::add(u, e) < O::add(d, r));
+    } else {
+        r = -O::log(RealOps<R>::u01(kOO, sw.at(pos)));
+        acc = true;
+    }
+    *out = O::mul(k.beta, r);
+    return acc;
+}
+
+// The scalar fallback of algorithms T, W and E on one warp: the warp
+// evaluates 32 consecutive attempts at a time and the accepted ones fill the
+// `left` outputs in attempt order, which is what the sequential loop of
+// gamma_scalar produces.  Returns the words consumed (all lanes agree).
+template <typename R, int ALG, class SW>
+__device__ uint64_t gamma_scalar_warp(const GammaParam<R> &k, SW &sw, uint64_t pos, uint64_t left, R *o)
+{
+    constexpr uint64_t WA = GammaAttemptWords<ALG>::value;
+    const uint32_t lane = threadIdx.x & 31;
+    uint64_t filled = 0, j0 = 0;
+    for (;;) {
+        R v;
+        const bool acc = gamma_attempt<R, ALG>(k, sw, pos + WA * (j0 + lane), &v);
+        const uint32_t m = __ballot_sync(0xffffffffu, acc);
+        const uint32_t rank = __popc(m & ((1u << lane) - 1u));
+        if (acc && filled + rank < left) o[filled + rank] = v;
+        const uint32_t cnt = __popc(m);
+        if (filled + cnt >= left) {
+            // the attempt that fills the last output: the (left - filled)-th
+            // accepted lane
+            const uint32_t need = static_cast<uint32_t>(left - filled);
+            uint32_t mm = m;
+            for (uint32_t q = 1; q < need; ++q) mm &= mm - 1;
+            const uint32_t last = __ffs(mm) - 1;
+            return WA * (j0 + last + 1);
+        }
+        filled += cnt;
+        j0 += 32;
+    }
+}
+
 template <typename R>
 struct GammaTraits {
     static constexpr int K = 8192 / static_cast<int>(sizeof(R));
@@ -585,11 +657,20 @@ __global__ void __launch_bounds__(THREADS, 3) k_gamma(G g, Ctr ctr0, uint32_t id
             smem, shr, &sh_pos);
         left -= m;
         o += m;
-        if (left && threadIdx.x == 0) {
-            ScalarWords<G, W> sw{&g, B, off};
-            uint64_t sp = pos;
-            for (uint64_t q = 0; q < left; ++q) o[q] = gamma_scalar<R, ALG>(k, sw, sp);
-            for (uint64_t q = pos; q < sp; ++q) eng.call(1, M);
+        if constexpr (ALG != 2) {
+            if (left && threadIdx.x < 32) {
+                ScalarWords<G, W> sw{&g, B, off};
+                const uint64_t used = gamma_scalar_warp<R, ALG>(k, sw, pos, left, o);
+                if (threadIdx.x == 0)
+                    for (uint64_t q = 0; q < used; ++q) eng.call(1, M);
+            }
+        } else {
+            if (left && threadIdx.x == 0) {
+                ScalarWords<G, W> sw{&g, B, off};
+                uint64_t sp = pos;
+                for (uint64_t q = 0; q < left; ++q) o[q] = gamma_scalar<R, ALG>(k, sw, sp);
+                for (uint64_t q = pos; q < sp; ++q) eng.call(1, M);
+            }
         }
         if (!blocks && threadIdx.x == 0) {
             *ctr_out = eng.ctr;
