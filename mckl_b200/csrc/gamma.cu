@@ -218,6 +218,27 @@ struct ScalarNormal {
     }
 };
 
+// Algorithm N's acceptance test of one attempt (uniform u, normal w with
+// v = 1 + c w > 0); *r = d v^3 when accepted.
+template <typename R>
+__device__ __forceinline__ bool gamma_n_accept(const GammaParam<R> &k, R u, R w, R v, R *r)
+{
+    using O = GOps<R>;
+    v = O::mul(O::mul(v, v), v);
+    const R w2 = O::mul(w, w);
+    R e = O::sub(static_cast<R>(1), O::mul(O::mul(O::k0331, w2), w2));
+    if (u < e) {
+        *r = O::mul(k.d, v);
+        return true;
+    }
+    e = O::add(O::div(w2, static_cast<R>(2)), O::mul(k.d, O::add(O::sub(static_cast<R>(1), v), O::log(v))));
+    if (O::log(u) < e) {
+        *r = O::mul(k.d, v);
+        return true;
+    }
+    return false;
+}
+
 // GammaDistribution::generate_{t,w,n,e} (:350-459), the scalar fallback.
 template <typename R, int ALG, class SW>
 __device__ R gamma_scalar(const GammaParam<R> &k, SW &sw, uint64_t &pos)
@@ -257,19 +278,7 @@ __device__ R gamma_scalar(const GammaParam<R> &k, SW &sw, uint64_t &pos)
                     w = rn(sw, pos);
                     v = O::add(static_cast<R>(1), O::mul(c, w));
                 } while (v <= 0);
-                v = O::mul(O::mul(v, v), v);
-                const R w2 = O::mul(w, w);
-                R e = O::sub(static_cast<R>(1), O::mul(O::mul(O::k0331, w2), w2));
-                if (u < e) {
-                    r = O::mul(d, v);
-                    break;
-                }
-                e = O::add(O::div(w2, static_cast<R>(2)),
-                    O::mul(d, O::add(O::sub(static_cast<R>(1), v), O::log(v))));
-                if (O::log(u) < e) {
-                    r = O::mul(d, v);
-                    break;
-                }
+                if (gamma_n_accept(k, u, w, v, &r)) break;
             }
             break;
         }
@@ -350,6 +359,54 @@ __device__ uint64_t gamma_scalar_warp(const GammaParam<R> &k, SW &sw, uint64_t p
         filled += cnt;
         j0 += 32;
     }
+}
+
+// The scalar fallback of algorithm N on one warp.  Each value draws with a
+// fresh scalar normal, so a value whose first attempt is accepted with
+// v = 1 + c w > 0 consumed exactly three words (its uniform and one
+// Box-Muller pair) -- a regular value.  Lane l evaluates value q0 + l as if
+// every value before it were regular (its words start at pos + 3 l); the
+// values before the first irregular lane are final, and the irregular value
+// is then drawn by lane 0 with the sequential loop from its (now known)
+// start.  Returns the position after the last value (all lanes agree).
+template <typename R, class G, class SW>
+__device__ uint64_t gamma_scalar_n_warp(const GammaParam<R> &k, SW &sw, uint64_t pos, uint64_t left, R *o)
+{
+    using O = GOps<R>;
+    const uint32_t lane = threadIdx.x & 31;
+    uint64_t q0 = 0;
+    while (q0 < left) {
+        const uint64_t q = q0 + lane;
+        const bool valid = q < left;
+        bool reg = false;
+        R val = 0;
+        if (valid) {
+            const uint64_t p = pos + 3 * static_cast<uint64_t>(lane);
+            const R u = RealOps<R>::u01(kOO, sw.at(p));
+            ScalarNormal<R> rn;
+            uint64_t pn = p + 1;
+            const R w = rn(sw, pn);
+            const R v = O::add(static_cast<R>(1), O::mul(k.c, w));
+            R r;
+            if (v > 0 && gamma_n_accept(k, u, w, v, &r)) {
+                reg = true;
+                val = O::mul(k.beta, r);
+            }
+        }
+        const uint32_t irr = __ballot_sync(0xffffffffu, valid && !reg);
+        const uint32_t nvalid = static_cast<uint32_t>(min(static_cast<uint64_t>(32), left - q0));
+        const uint32_t L = irr ? static_cast<uint32_t>(__ffs(irr) - 1) : nvalid;  // regular values this round
+        if (lane < L) o[q] = val;
+        pos += 3 * static_cast<uint64_t>(L);
+        q0 += L;
+        if (irr) {
+            uint64_t sp = pos;
+            if (lane == 0) o[q0] = gamma_scalar<R, 2>(k, sw, sp);
+            pos = __shfl_sync(0xffffffffu, sp, 0);
+            q0 += 1;
+        }
+    }
+    return pos;
 }
 
 template <typename R>
@@ -665,11 +722,11 @@ __global__ void __launch_bounds__(THREADS, 3) k_gamma(G g, Ctr ctr0, uint32_t id
                     for (uint64_t q = 0; q < used; ++q) eng.call(1, M);
             }
         } else {
-            if (left && threadIdx.x == 0) {
+            if (left && threadIdx.x < 32) {
                 ScalarWords<G, W> sw{&g, B, off};
-                uint64_t sp = pos;
-                for (uint64_t q = 0; q < left; ++q) o[q] = gamma_scalar<R, ALG>(k, sw, sp);
-                for (uint64_t q = pos; q < sp; ++q) eng.call(1, M);
+                const uint64_t sp = gamma_scalar_n_warp<R, G>(k, sw, pos, left, o);
+                if (threadIdx.x == 0)
+                    for (uint64_t q = pos; q < sp; ++q) eng.call(1, M);
             }
         }
         if (!blocks && threadIdx.x == 0) {
