@@ -128,7 +128,12 @@ size_t g_stage_words = 0;
 uint64_t *stage_words(size_t words)
 {
     if (words > g_stage_words) {
-        if (g_stage) cudaFreeHost(g_stage);
+        if (g_stage) {
+            // a call that failed after queuing its upload may still have
+            // it in flight from the old buffer
+            cudaDeviceSynchronize();
+            cudaFreeHost(g_stage);
+        }
         g_stage = nullptr;
         g_stage_words = 0;
         const size_t want = std::max<size_t>(words, 4096);
