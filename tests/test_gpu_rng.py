@@ -53,7 +53,11 @@ def ulps(a, b):
 def test_rand_streams(env, kind):
     mb, orc = env
     M = O.WORDS_PER_BLOCK[kind]
-    for (ctr, idx) in (((0,), None), ((5,), 0), ((7,), 1), ((9,), M - 1), ((2**64 - 2, 3), None), ((2**64 - 1,), 1)):
+    # low counter words that do and do not carry into bit 32 within a call
+    # (the Philox fill folds the block-independent rounds only when they do
+    # not), and nonzero upper words
+    for (ctr, idx) in (((0,), None), ((5,), 0), ((7,), 1), ((9,), M - 1), ((2**64 - 2, 3), None), ((2**64 - 1,), 1),
+                       ((2**32 - 3,), None), ((2**33 + 7, 12345), None), ((2**40 + 3, 2**50 + 9), 2)):
         for n in (0, 1, 3, 5, 17, 1000, 4096 * 3 + 5, 1 << 20):
             g, e = pair(mb, kind, key=(42, 5, 3, 1), ctr=ctr, index=idx)
             want = orc.rand(e, n)
@@ -100,12 +104,13 @@ def test_u01_bit_exact(env, kind):
            "co": mb.u01_co_distribution, "oc": mb.u01_oc_distribution, "oo": mb.u01_oo_distribution}
     for var, fn in fns.items():
         for dt in ("f32", "f64"):
-            for (idx, n) in ((None, 5000), (1, 4099), (2, 1 << 18)):
-                g, e = pair(mb, kind, ctr=(3,), index=idx)
+            for (ctr, idx, n) in (((3,), None, 5000), ((3,), 1, 4099), ((3,), 2, 1 << 18), ((2**32 - 700,), None, 5000),
+                                  ((2**35 + 1, 7), None, 4096 * 4 + 12)):
+                g, e = pair(mb, kind, ctr=ctr, index=idx)
                 want = orc.u01(e, var, dt == "f64", n)
                 got = fn(g, n, dtype=dt).cpu().numpy()
-                assert np.array_equal(got.view(np.uint8), want.view(np.uint8)), (var, dt, idx, n)
-                assert same_state(g, e), (var, dt, idx, n)
+                assert np.array_equal(got.view(np.uint8), want.view(np.uint8)), (var, dt, ctr, idx, n)
+                assert same_state(g, e), (var, dt, ctr, idx, n)
 
 
 @pytest.mark.parametrize("kind", range(1, 7))
