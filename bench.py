@@ -258,7 +258,7 @@ def bench_smc(args, rank, world, dev):
     extra = {"autotune": [{"threads": t, "ctas_per_sm": c, "ms": round(m, 3)} for (t, c, m) in trials],
              "resampling_events_per_step": int(nres.sum())}
     if rank == 0:
-        import oracle as O
+        from mckl_b200.kalman import kalman_ar1
 
         bs = make_filters(mb, w, shadow=True, threshold=args.threshold)
         best = min(trials, key=lambda r: r[2])
@@ -268,8 +268,7 @@ def bench_smc(args, rank, world, dev):
         ll64 = bs.shadow_loglik()
         bs.close()
         rel = np.abs(ll32 - ll64) / np.abs(ll64)
-        orc = O.CPUPath("oracle")
-        kf = np.array([orc.kalman_ar1(w["y"][f], w["phi"][f], w["sx"][f], w["sy"][f])[0] for f in range(len(w["N"]))])
+        kf, _ = kalman_ar1(w["y"], w["phi"], w["sx"], w["sy"])
         extra["accuracy"] = {
             "fp32_vs_fp64_same_genealogy_rel": {"max": float(rel.max()), "median": float(np.median(rel)),
                                                 "frac_le_1e-6": float(np.mean(rel <= 1e-6))},
@@ -359,6 +358,72 @@ def bench_callers(dev, hbm_peak, peak_kind, reps=5):
     return out
 
 
+def bench_plain_c3(N=1 << 20, T=1000):
+    """The plain FP64 particle filter (the reference's step order, one
+    filter): N = 2^20 particles, T = 1000 observations simulated from
+    Philox4x32 key (7, 0) (x_0 ~ N(0, 1 / 0.19), phi = 0.9, sx = 1, sy = 0.5),
+    systematic resampling at ESS < N / 2; wall clock with the device
+    synchronised (the step loop is host-driven), and the estimate against
+    the exact Kalman log-likelihood."""
+    import numpy as np
+    import torch
+
+    import mckl_b200 as mb
+    from mckl_b200.kalman import kalman_ar1
+
+    phi, sx, sy = 0.9, 1.0, 0.5
+    sd0 = sx / np.sqrt(1 - phi * phi)
+    g = mb.Philox4x32()
+    g.key = (7, 0)
+    z = mb.normal_distribution(g, 2 * T + 2).cpu().numpy()
+    x = sd0 * z[0]
+    y = np.zeros(T + 1)
+    for t in range(1, T + 1):
+        x = phi * x + sx * z[t]
+        y[t] = x + sy * z[T + t]
+    mb.pf_ar1_plain(N, y[:11], phi, sx, sy, sd0, (11, 0), (12, 0), scheme=mb.Systematic)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = mb.pf_ar1_plain(N, y, phi, sx, sy, sd0, (11, 0), (12, 0), scheme=mb.Systematic)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    kf, _ = kalman_ar1(y, phi, sx, sy)
+    return {"workload": "plain FP64 particle filter, N = 2^20, T = 1000, systematic resampling at ESS < N/2",
+            "particle_steps_per_s": N * T / dt, "s": round(dt, 3), "resampling_steps": int(res["resampled"].sum()),
+            "loglik": res["loglik"], "loglik_minus_kalman": float(res["loglik"] - kf[0]),
+            "bound": "host round trip per step (the reference's step order: normaliser and ESS read back)",
+            "y": y}
+
+
+def cpu_c3_reference(y, N=1 << 20, T=30):
+    """The compiled reference's SMCSampler (BackendSEQ, one thread) on the
+    same model: N = 2^20 particles, the first T observations."""
+    import numpy as np
+
+    import oracle as O
+
+    if not O.have_ref():
+        return None
+    cpu = O.CPUPath("ref")
+    Nv = np.array([N], dtype=np.uint64)
+    yy = np.ascontiguousarray(y[:T + 1][None, :])
+    phi, sx, sy = (np.array([v]) for v in (0.9, 1.0, 0.5))
+    mk = np.array([[11, 0]], dtype=np.uint32)
+    rk = np.array([[12, 0]], dtype=np.uint32)
+    ll = np.zeros(1)
+
+    def p(a):
+        return ctypes.c_void_p(a.ctypes.data)
+
+    t0 = time.perf_counter()
+    rc = cpu._pf_ar1_batch(1, p(Nv), T, p(yy), p(phi), p(sx), p(sy), p(mk), p(rk), 2, 0.5, p(ll), 1)
+    dt = time.perf_counter() - t0
+    if rc != 0:
+        return None
+    return {"value": N * T / dt, "unit": "particle-steps/s", "cores": 1, "kind": "reference",
+            "sample": f"N = 2^20, the first {T} of the 1000 steps; {dt:.1f} s"}
+
+
 def cpu_callers_reference():
     """The compiled reference's ResampleIndex::read_index_matrix (one thread)
     on N = 2^16, R = 100 (push_back copies included)."""
@@ -388,8 +453,8 @@ def bench_adjoint(rank, dev, sets=256, N=1 << 16, T=1000, C=32, threads=512):
     import torch
 
     import mckl_b200 as mb
-    import oracle as O
     from mckl_b200 import autograd as AG
+    from mckl_b200.kalman import kalman_ar1
 
     w = mb.batched_workload(F=sets, T=T, seed=4321 + 7919 * rank, nmin=N, nmax=N + 1)
     b = mb.BatchedFilters(w["N"], w["y"], w["phi"], w["sx"], w["sy"], w["mkeys"], w["rkeys"], fp64=True)
@@ -411,11 +476,7 @@ def bench_adjoint(rank, dev, sets=256, N=1 << 16, T=1000, C=32, threads=512):
     fd2 = AG.finite_differences(w, h=5e-6, threads=threads)
     rich = (4.0 * fd2 - fd) / 3.0
     rel_rich = np.abs(g - rich) / np.maximum(np.abs(rich), 1.0)
-    orc = O.CPUPath("oracle")
-    kg = np.zeros_like(g)
-    kll = np.zeros(sets)
-    for f in range(sets):
-        kll[f], kg[f] = orc.kalman_ar1(w["y"][f], w["phi"][f], w["sx"][f], w["sy"][f])
+    kll, kg = kalman_ar1(w["y"], w["phi"], w["sx"], w["sy"])
     rel_k = np.linalg.norm(g - kg, axis=1) / np.linalg.norm(kg, axis=1)
     cos = np.sum(g * kg, axis=1) / (np.linalg.norm(g, axis=1) * np.linalg.norm(kg, axis=1))
     ps = float(sets) * N * T
@@ -809,6 +870,11 @@ def main():
                                             ph / rng["philox_c1"]["store_only_fill_2^26"]["GB_s"]}}
             if rank == 0:
                 line["callers"] = bench_callers(dev, hbm_peak, peak_kind)
+                c3 = bench_plain_c3()
+                y3 = c3.pop("y")
+                if world == 1:
+                    c3["cpu_reference"] = cpu_c3_reference(y3)
+                line["plain_c3"] = c3
             if rank == 0 and world == 1:
                 cc = cpu_callers_reference()
                 if cc:

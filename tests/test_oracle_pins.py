@@ -204,3 +204,22 @@ def test_weighted_estimate_oracle_pin():
             bound = n * 2.0**-53 * float(np.sum(np.abs(W * u[:, j])))
             assert abs(got[j] - math.fsum(W * u[:, j])) <= bound
             assert abs(got[j] - lib[j]) <= 2 * bound
+
+
+def test_library_kalman_matches_oracle():
+    """The package's vectorised Kalman filter (the yardstick the bench
+    reports against) equals the oracle's scalar one."""
+    from mckl_b200.kalman import kalman_ar1
+
+    orc = O.CPUPath("oracle")
+    rng = np.random.default_rng(8)
+    F, T = 5, 200
+    y = rng.normal(size=(F, T + 1))
+    phi = rng.uniform(0.5, 0.99, F)
+    sx = rng.uniform(0.5, 2, F)
+    sy = rng.uniform(0.2, 1, F)
+    ll, g = kalman_ar1(y, phi, sx, sy)
+    for f in range(F):
+        l1, g1 = orc.kalman_ar1(y[f], phi[f], sx[f], sy[f])
+        assert abs(ll[f] - l1) <= 1e-10 * abs(l1)
+        assert np.allclose(g[f], g1, rtol=1e-9, atol=1e-9)
