@@ -360,6 +360,9 @@ class ResampleIndex:
 
     def __init__(self):
         self._v = []
+        self._ptr = []  # device addresses and sizes of the vectors, kept beside them
+        self._len = []
+        self._arrays = {}  # (first, last) -> ctypes address / size arrays of that range
 
     def num_iter(self):
         return len(self._v)
@@ -371,6 +374,9 @@ class ResampleIndex:
 
     def reset(self):
         self._v = []
+        self._ptr = []
+        self._len = []
+        self._arrays = {}
 
     def push_back(self, N, index=None):
         """Append the parent indices of one iteration (a CUDA int64/uint64
@@ -380,16 +386,25 @@ class ResampleIndex:
             index = torch.arange(N, dtype=torch.int64, device="cuda")
         if index.numel() != N or not index.is_cuda or index.element_size() != 8:
             raise ValueError("index: CUDA tensor of N 64-bit integers")
-        self._v.append(index.contiguous())
+        v = index.contiguous()
+        self._v.append(v)
+        self._ptr.append(v.data_ptr())
+        self._len.append(v.numel())
 
-    def _run(self, vecs, col_major):
+    def _run(self, rows, col_major):
+        """rows: the vector numbers, oldest first (the last is the one whose
+        particles the result describes)."""
         torch = _torch()
-        R = len(vecs)
-        N = int(vecs[-1].numel())
+        key = tuple(rows)
+        arr = self._arrays.get(key)
+        if arr is None:
+            arr = ((ctypes.c_uint64 * len(rows))(*[self._ptr[r] for r in rows]),
+                   (ctypes.c_size_t * len(rows))(*[self._len[r] for r in rows]))
+            self._arrays = {key: arr}  # one range kept: the usual caller repeats it
+        R = len(rows)
+        N = int(self._len[rows[-1]])
         out = torch.empty(N * R, dtype=torch.int64, device="cuda")
-        ptrs = (ctypes.c_uint64 * R)(*[v.data_ptr() for v in vecs])
-        sizes = (ctypes.c_size_t * R)(*[v.numel() for v in vecs])
-        _check(_index_matrix(N, R, ctypes.cast(ptrs, _vp), ctypes.cast(sizes, _vp), int(col_major),
+        _check(_index_matrix(N, R, ctypes.cast(arr[0], _vp), ctypes.cast(arr[1], _vp), int(col_major),
                              ctypes.c_void_p(out.data_ptr()), _stream_ptr()))
         return out
 
@@ -399,7 +414,7 @@ class ResampleIndex:
         ib = self.num_iter() - 1 if iter_back is None else iter_back
         if not (0 <= iter_ <= ib < self.num_iter()):
             raise IndexError("iteration numbers out of range")
-        return self._run(self._v[iter_:ib + 1], layout == self.ColMajor)
+        return self._run(list(range(iter_, ib + 1)), layout == self.ColMajor)
 
     def index(self, id_, iter_back=None, iter_=0):
         """index(id, iter_back, iter) (:666-678): from the last iteration's
@@ -407,8 +422,7 @@ class ResampleIndex:
         ib = self.num_iter() - 1 if iter_back is None else iter_back
         if not (0 <= iter_ <= ib < self.num_iter()):
             raise IndexError("iteration numbers out of range")
-        vecs = self._v[iter_:ib] + [self._v[-1]]
-        col = self._run(vecs, True)
+        col = self._run(list(range(iter_, ib)) + [self.num_iter() - 1], True)
         return int(col[id_].item())
 
 
