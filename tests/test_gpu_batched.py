@@ -116,3 +116,34 @@ def test_batched_autotune_and_set_y(env, small):
     assert not np.array_equal(ll2, ll)
     for h in (b, ref, c):
         h.close()
+
+
+def test_batched_ragged_particle_counts(env):
+    """Particle counts around every boundary of the kernel's layout: one
+    particle, odd counts, the 32-particle alignment of filter ranges, the
+    1024-value noise chunks, the 2048-particle resampling tiles of 256
+    threads and the 4096 of 512 threads; FP64 against the plain filter and
+    FP32 against its FP64 shadow."""
+    mb, _ = env
+    Ns = [1, 2, 3, 5, 31, 32, 33, 255, 257, 1023, 1024, 1025, 2047, 2049, 4095, 4097]
+    w = mb.batched_workload(F=len(Ns), T=50, seed=77, nmin=256, nmax=512)
+    w["N"] = np.array(Ns, dtype=np.uint64)
+    for threads, cps in ((256, 4), (512, 2)):
+        b = mb.BatchedFilters(w["N"], w["y"], w["phi"], w["sx"], w["sy"], w["mkeys"], w["rkeys"], fp64=True)
+        b.config(threads=threads, ctas_per_sm=cps)
+        b.run()
+        ll, nr = b.results()
+        b.close()
+        close = 0
+        for f in range(len(Ns)):
+            lp, npl = plain(mb, w, f)
+            assert nr[f] == npl, (threads, Ns[f])
+            close += abs(ll[f] - lp) <= 1e-9 * abs(lp)
+        assert close >= len(Ns) - 1, (threads, close)
+        b = mb.BatchedFilters(w["N"], w["y"], w["phi"], w["sx"], w["sy"], w["mkeys"], w["rkeys"], shadow=True)
+        b.config(threads=threads, ctas_per_sm=cps)
+        b.run()
+        ll, _ = b.results()
+        rel = np.abs(ll - b.shadow_loglik()) / np.abs(b.shadow_loglik())
+        b.close()
+        assert rel.max() <= 1e-6, (threads, rel)
