@@ -22,19 +22,7 @@ namespace {
 // Every thread follows kLines particle lines at once (particles i, i + S, ..,
 // S the grid's thread count), so kLines dependent gathers are in flight per
 // thread.
-#ifndef MB_GEN_LINES
-#define MB_GEN_LINES 2
-#endif
-#ifndef MB_GEN_MINB
-#define MB_GEN_MINB 8
-#endif
-#ifndef MB_GEN_ROW_TILE
-#define MB_GEN_ROW_TILE 8
-#endif
-#ifndef MB_GEN_ROW_LINES
-#define MB_GEN_ROW_LINES 1
-#endif
-constexpr int kLines = MB_GEN_LINES;
+constexpr int kLines = 2;  // 1, 4 and 8 measured slower
 
 // one step back along a line: a parent index outside the earlier vector would
 // read past it, so it records the error and stops the line
@@ -51,7 +39,7 @@ __device__ __forceinline__ void step_back(uint64_t r, uint64_t R, const uint64_t
     }
 }
 
-__global__ void __launch_bounds__(256, MB_GEN_MINB) k_index_matrix_cols(uint64_t N, uint64_t R, const uint64_t *const *index,
+__global__ void __launch_bounds__(256, 8) k_index_matrix_cols(uint64_t N, uint64_t R, const uint64_t *const *index,
     const uint64_t *sizes, uint64_t *out, uint32_t *err)
 {
     const uint64_t S = static_cast<uint64_t>(gridDim.x) * blockDim.x;
@@ -77,8 +65,8 @@ __global__ void __launch_bounds__(256, MB_GEN_MINB) k_index_matrix_cols(uint64_t
 // row-major: a CTA owns 256 * kRowLines consecutive particles and stages
 // kRowTile iterations of their lines in shared memory, then writes each
 // particle's kRowTile contiguous words with consecutive threads
-constexpr int kRowTile = MB_GEN_ROW_TILE;
-constexpr int kRowLines = MB_GEN_ROW_LINES;
+constexpr int kRowTile = 8;   // 16 measured slower
+constexpr int kRowLines = 1;  // 2 measured slower
 constexpr int kRowParts = 256 * kRowLines;
 
 __global__ void __launch_bounds__(256) k_index_matrix_rows(uint64_t N, uint64_t R, const uint64_t *const *index,
