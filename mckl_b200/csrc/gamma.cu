@@ -28,6 +28,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "block_scan.cuh"
 #include "common.cuh"
 #include "dispatch.cuh"
 #include "transforms.cuh"
@@ -166,27 +167,43 @@ struct ScalarWords {
     }
 };
 
-// CTA-wide rank of a predicate in thread order: returns the number of
-// threads below this one with f set; *total gets the CTA count.  `sh` holds
-// one word per warp plus one.
-template <int THREADS>
-__device__ __forceinline__ uint32_t block_rank(bool f, uint32_t *sh, uint32_t *total)
+// CTA-wide ranks of E predicates per thread in index order, element (t, j)
+// having index t + j THREADS: rank[j] = the number of set elements with a
+// smaller index, *total the CTA count.  Three barriers for all E (one ballot
+// per j; warp 0 scans the E x warps counts).  `sh` holds E THREADS / 32 + 1
+// words (at most 64 + 1).
+template <int THREADS, int E>
+__device__ __forceinline__ void block_rank_multi(const bool (&f)[E], uint32_t *sh, uint32_t (&rank)[E],
+    uint32_t *total)
 {
-    constexpr int NW = THREADS / 32;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t b = __ballot_sync(0xffffffffu, f);
-    if (lane == 0) sh[warp] = __popc(b);
-    __syncthreads();
-    uint32_t before = 0, tot = 0;
+    constexpr int NW = THREADS / 32, L = E * NW;
+    static_assert(L <= 64, "two counts per lane of warp 0");
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t b[E];
 #pragma unroll
-    for (int w = 0; w < NW; ++w) {
-        const uint32_t c = sh[w];
-        before += (w < warp) ? c : 0u;
-        tot += c;
+    for (int j = 0; j < E; ++j) {
+        b[j] = __ballot_sync(0xffffffffu, f[j]);
+        if (lane == 0) sh[j * NW + warp] = __popc(b[j]);
     }
     __syncthreads();
-    *total = tot;
-    return before + __popc(b & ((1u << lane) - 1u));
+    if (warp == 0) {
+        const uint32_t a0 = lane < static_cast<uint32_t>(L) ? sh[lane] : 0u;
+        const uint32_t a1 = lane + 32 < static_cast<uint32_t>(L) ? sh[lane + 32] : 0u;
+        const uint32_t s0 = warp_inclusive_sum(a0);
+        const uint32_t t0 = __shfl_sync(0xffffffffu, s0, 31);
+        const uint32_t s1 = warp_inclusive_sum(a1) + t0;
+        const uint32_t t1 = __shfl_sync(0xffffffffu, s1, 31);
+        __syncwarp();
+        if (lane < static_cast<uint32_t>(L)) sh[lane] = s0 - a0;
+        if (lane + 32 < static_cast<uint32_t>(L)) sh[lane + 32] = s1 - a1;
+        if (lane == 0) sh[L] = t1;
+    }
+    __syncthreads();
+    const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int j = 0; j < E; ++j) rank[j] = sh[j * NW + warp] + __popc(b[j] & lt);
+    *total = sh[L];
+    __syncthreads();  // `sh` is rewritten by the next call
 }
 
 // Scalar normal with the cached second variate (random/normal_distribution.hpp:136-153).
@@ -536,15 +553,17 @@ __device__ uint32_t gamma_chunk(const G &g, const GammaParam<R> &k, const Ctr &B
         R *lv = lw + K;
         int rk[EPT];
         uint32_t nred = 0;
+        {
+            bool f[EPT];
+            uint32_t r[EPT];
 #pragma unroll
-        for (int j = 0; j < EPT; ++j) {
-            const uint32_t i = threadIdx.x + j * THREADS;
-            const bool f = i < n && v[j] <= 0;
-            uint32_t tot;
-            const uint32_t r = block_rank<THREADS>(f, shr, &tot);  // syncs: staging reads are done
-            rk[j] = f ? static_cast<int>(nred + r) : -1;
-            if (f) lidx[nred + r] = i;
-            nred += tot;
+            for (int j = 0; j < EPT; ++j) f[j] = threadIdx.x + j * THREADS < n && v[j] <= 0;
+            block_rank_multi<THREADS, EPT>(f, shr, r, &nred);  // syncs: staging reads are done
+#pragma unroll
+            for (int j = 0; j < EPT; ++j) {
+                rk[j] = f[j] ? static_cast<int>(r[j]) : -1;
+                if (f[j]) lidx[r[j]] = threadIdx.x + j * THREADS;
+            }
         }
         if (nred) {
             __syncthreads();
@@ -652,14 +671,11 @@ __device__ uint32_t gamma_chunk(const G &g, const GammaParam<R> &k, const Ctr &B
     }
     if constexpr (ALG == 3) return got;
     // ---- compaction of the accepted values, in index order
-    uint32_t m = 0;
+    uint32_t m = 0, r[EPT];
+    block_rank_multi<THREADS, EPT>(acc, shr, r, &m);
 #pragma unroll
-    for (int j = 0; j < EPT; ++j) {
-        uint32_t tot;
-        const uint32_t r = block_rank<THREADS>(acc[j], shr, &tot);
-        if (acc[j]) out[m + r] = x[j];
-        m += tot;
-    }
+    for (int j = 0; j < EPT; ++j)
+        if (acc[j]) out[r[j]] = x[j];
     return m;
 }
 
@@ -678,7 +694,7 @@ __global__ void __launch_bounds__(THREADS, 3) k_gamma(G g, Ctr ctr0, uint32_t id
     using S = GammaSmem<G, W, R>;
     constexpr int K = S::K;
     constexpr uint32_t M = static_cast<uint32_t>(S::WPB);
-    __shared__ uint32_t shr[THREADS / 32 + 1];
+    __shared__ uint32_t shr[THREADS / 32 * GammaTraits<float>::K / THREADS + 1];
     __shared__ uint64_t sh_pos;
     extern __shared__ __align__(16) unsigned char gamma_dyn[];
     g.prepare();
