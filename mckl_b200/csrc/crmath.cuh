@@ -10,9 +10,10 @@
 // agree with the reference to within its own rounding.
 //
 // Methods (standard, written from the mathematics):
-//   log: x = 2^e m, m in [1/sqrt2, sqrt2); log m = 2 atanh(z), z = (m-1)/(m+1),
-//        atanh series in z^2 (|z| <= 0.1716) with its first terms in
-//        double-double; e ln2 with ln2 as a double-double constant.
+//   log: x = 2^e m, m in [1, 2); a 128-entry table gives inv ~ 1/m with
+//        nine bits and -ln(inv) in double-double, r = m inv - 1 exactly,
+//        log1p(r) by its series (|r| <= 2^-7); e ln2 with ln2 as a
+//        double-double constant.
 //   exp: x = k ln2 + r (Cody-Waite, three-part ln2), r/16 through a Taylor
 //        series for expm1 in double-double, four squarings of 1 + expm1,
 //        scaled by 2^k.
@@ -137,7 +138,31 @@ constexpr double kLn2Hi = 0x1.62e42fefa39efp-1, kLn2Lo = 0x1.abc9e3b39803fp-56;
 constexpr double kThirdHi = 0x1.5555555555555p-2, kThirdLo = 0x1.5555555555555p-56;
 constexpr double kSqrt2 = 0x1.6a09e667f3bcdp+0;
 
+// Reduction table of log: {inv_i, -ln(inv_i) hi, lo} (log_table.inc, written
+// by gen_log_table.py).  Device copy in global memory (the lanes of a warp
+// index it at random: a constant-bank copy would serialise them).
+#if defined(__CUDACC__)
+static __device__ const double kLogTab[128][3] = {
+#include "log_table.inc"
+};
+#endif
+#if !defined(__CUDA_ARCH__)
+static const double kLogTabHost[128][3] = {
+#include "log_table.inc"
+};
+#endif
+#if defined(__CUDA_ARCH__)
+#define MB_LOGTAB(i, k) __ldg(&kLogTab[(i)][(k)])
+#else
+#define MB_LOGTAB(i, k) kLogTabHost[(i)][(k)]
+#endif
+
 // Correctly rounded (see header) natural logarithm of a double.
+// x = 2^e m, m in [1, 2); the top seven fraction bits pick inv_i ~ 1/m with
+// nine significant bits, so r = m inv_i - 1 is exact (one fma) and
+// |r| <= 2^-7; log x = e ln2 + (-ln inv_i) + log1p(r), with
+// log1p(r) = r - r^2/2 + r^3 P(r), P the series sum_{n>=3} (-1)^(n+1) r^(n-3)/n
+// to n = 12 in double, the rest in double-double.
 MB_HD double log(double x)
 {
     if (!(x > 0.0)) return x == 0.0 ? -MB_FROM_BITS(0x7ff0000000000000ll) : MB_FROM_BITS(0x7ff8000000000000ll);
@@ -152,43 +177,29 @@ MB_HD double log(double x)
     } else {
         e = ex - 1023;
     }
-    double m = MB_FROM_BITS((bits & 0x000fffffffffffffll) | 0x3ff0000000000000ll);
-    if (m > kSqrt2) {
-        m = MB_MUL(m, 0.5);
-        e += 1;
-    }
-    const double r = MB_SUB(m, 1.0);  // exact (Sterbenz)
-    const DD d = two_sum(m, 1.0);
-    const double inv = MB_DIV(1.0, d.hi);
-    const double zh = MB_MUL(r, inv);  // any rounding of zh is absorbed by the correction
-    double t = MB_FMA(-zh, d.hi, r);
-    t = MB_FMA(-zh, d.lo, t);
-    const DD z = fast_two_sum(zh, MB_MUL(t, inv));
-    const DD w = mul(z, z);
-    const double wh = w.hi;
-    // U = sum_{k=0}^{11} w^k / (2k + 5)
-    double U = 0x1.2f684bda12f68p-5;
-    U = MB_FMA(U, wh, 0x1.47ae147ae147bp-5);
-    U = MB_FMA(U, wh, 0x1.642c8590b2164p-5);
-    U = MB_FMA(U, wh, 0x1.8618618618618p-5);
-    U = MB_FMA(U, wh, 0x1.af286bca1af28p-5);
-    U = MB_FMA(U, wh, 0x1.e1e1e1e1e1e1ep-5);
-    U = MB_FMA(U, wh, 0x1.1111111111111p-4);
-    U = MB_FMA(U, wh, 0x1.3b13b13b13b14p-4);
-    U = MB_FMA(U, wh, 0x1.745d1745d1746p-4);
-    U = MB_FMA(U, wh, 0x1.c71c71c71c71cp-4);
-    U = MB_FMA(U, wh, 0x1.2492492492492p-3);
-    U = MB_FMA(U, wh, 0x1.999999999999ap-3);
-    const DD T = add(DD{kThirdHi, kThirdLo}, mul_d(w, U));  // 1/3 + w U
-    const DD S = add_d(mul(w, T), 1.0);                      // 1 + w T
-    DD lm = mul(z, S);
-    lm.hi = MB_MUL(lm.hi, 2.0);
-    lm.lo = MB_MUL(lm.lo, 2.0);
+    const double m = MB_FROM_BITS((bits & 0x000fffffffffffffll) | 0x3ff0000000000000ll);
+    const int i = static_cast<int>((bits >> 45) & 127);
+    const double r = MB_FMA(m, MB_LOGTAB(i, 0), -1.0);  // exact
+    double P = -0x1.5555555555555p-4;                   // -1/12
+    P = MB_FMA(P, r, 0x1.745d1745d1746p-4);             // 1/11
+    P = MB_FMA(P, r, -0x1.999999999999ap-4);            // -1/10
+    P = MB_FMA(P, r, 0x1.c71c71c71c71cp-4);             // 1/9
+    P = MB_FMA(P, r, -0x1.0000000000000p-3);            // -1/8
+    P = MB_FMA(P, r, 0x1.2492492492492p-3);             // 1/7
+    P = MB_FMA(P, r, -0x1.5555555555555p-3);            // -1/6
+    P = MB_FMA(P, r, 0x1.999999999999ap-3);             // 1/5
+    P = MB_FMA(P, r, -0x1.0000000000000p-2);            // -1/4
+    P = MB_FMA(P, r, 0x1.5555555555555p-2);             // 1/3
+    const DD r2 = two_prod(r, r);
+    const double r3p = MB_MUL(MB_MUL(r2.hi, r), P);
+    DD lp = two_sum(r, MB_MUL(r2.hi, -0.5));
+    lp.lo = MB_ADD(lp.lo, MB_ADD(MB_MUL(r2.lo, -0.5), r3p));
+    lp = fast_two_sum(lp.hi, lp.lo);
     const double ed = static_cast<double>(e);
     DD el = two_prod(ed, kLn2Hi);
     el.lo = MB_FMA(ed, kLn2Lo, el.lo);
     el = fast_two_sum(el.hi, el.lo);
-    const DD res = add(el, lm);
+    const DD res = add(add(el, DD{MB_LOGTAB(i, 1), MB_LOGTAB(i, 2)}), lp);
     return MB_ADD(res.hi, res.lo);
 }
 
