@@ -388,7 +388,7 @@ def bench_plain_c3(N=1 << 20, T=1000):
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
     kf, _ = kalman_ar1(y, phi, sx, sy)
-    return {"workload": "plain FP64 particle filter, N = 2^20, T = 1000, systematic resampling at ESS < N/2",
+    return {"workload": f"plain FP64 particle filter, N = 2^20, T = {T}, systematic resampling at ESS < N/2",
             "particle_steps_per_s": N * T / dt, "s": round(dt, 3), "resampling_steps": int(res["resampled"].sum()),
             "loglik": res["loglik"], "loglik_minus_kalman": float(res["loglik"] - kf[0]),
             "bound": "host round trip per step (the reference's step order: normaliser and ESS read back)",
@@ -753,8 +753,9 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mckl_b200", choices=["mckl_b200", "reference"])
-    ap.add_argument("--workload", default="smc", choices=["smc", "rng", "callers"],
-                    help="callers: only the index matrix / weighted estimate / PMCMC measurements, one JSON object")
+    ap.add_argument("--workload", default="smc", choices=["smc", "rng", "callers", "plain"],
+                    help="callers: only the index matrix / weighted estimate / PMCMC measurements; plain: only the "
+                         "plain FP64 filter at N = 2^20 (T = --obs, 1000 by default); one JSON object each")
     ap.add_argument("--filters", type=int, default=4096)
     ap.add_argument("--obs", type=int, default=500)
     ap.add_argument("--parts", default="all", choices=["all", "timed"])
@@ -817,6 +818,15 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     hbm_peak, sm_max, peak_kind = measured_peaks()
+    if args.workload == "plain":
+        if rank == 0:
+            T = args.obs if args.obs != 500 else 1000
+            c3 = bench_plain_c3(T=T)
+            c3.pop("y")
+            print(json.dumps({"workload": "plain", "n_gpus": 1, "plain_c3": c3}))
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
     if args.workload == "callers":
         if rank == 0:
             out = {"workload": "callers", "n_gpus": 1, "callers": bench_callers(dev, hbm_peak, peak_kind)}
