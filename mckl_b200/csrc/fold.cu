@@ -13,6 +13,7 @@ constexpr int kDescThreads = 256;
 constexpr int kPer = kFoldTile / kDescThreads;  // 16 consecutive elements per thread
 constexpr int kWalkThreads = 1024;
 constexpr int kWalkPer = kFoldTile / kWalkThreads;  // 4
+constexpr unsigned kSeqStretch = 256;  // elements folded one at a time after two scan rounds of a tile
 
 __device__ __forceinline__ double ulp_of(double v)
 {
@@ -98,7 +99,29 @@ __device__ double fold_tile_exact(const double *x, uint64_t len, double s, doubl
 #pragma unroll
     for (int k = 0; k < kWalkPer; ++k) xr[k] = (static_cast<uint64_t>(j0 + k) < len) ? x[j0 + k] : 0.0;
     unsigned cur = 0;
+    int rounds = 0;  // scan rounds since the last sequential stretch
     while (cur < len) {
+        if (rounds >= 2) {
+            // events are dense here (the first tiles cross a binade every few
+            // elements): the next kSeqStretch elements one at a time, by one
+            // thread, cost less than a CTA scan per event
+            const unsigned end = static_cast<unsigned>(std::min<uint64_t>(len, cur + kSeqStretch));
+            if (threadIdx.x == 0) {
+                double v = s;
+                for (unsigned j = cur; j < end; ++j) {
+                    v = __dadd_rn(v, x[j]);
+                    if (prefix) prefix[j] = v;
+                }
+                sh_next = v;
+            }
+            __syncthreads();
+            s = sh_next;
+            __syncthreads();
+            cur = end;
+            rounds = 0;
+            continue;
+        }
+        ++rounds;
         if (s == 0.0) {
             // nothing accumulated yet: the next sum is exact, 0 + x = x
             if (static_cast<unsigned>(j0) <= cur && cur < static_cast<unsigned>(j0 + kWalkPer)) {
