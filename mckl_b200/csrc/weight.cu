@@ -54,27 +54,49 @@ __global__ void k_weight_exp(uint64_t N, double *W, const long long *lmax_bits)
     }
 }
 
-// one thread per chunk: that chunk's ddot fold
-__global__ void k_weight_chunkdot(uint64_t N, const double *W, double *dots)
+// one warp per chunk: the lanes form the chunk's products w_i^2 (each
+// rounded once, independent of the others) with coalesced loads into shared
+// memory, then lane 0 adds them in index order -- that chunk's ddot fold
+constexpr int kDotWarps = 4;
+
+__global__ void __launch_bounds__(32 * kDotWarps) k_weight_chunkdot(uint64_t N, const double *W, double *dots)
 {
-    const uint64_t c = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    __shared__ double sq[kDotWarps][kChunk];
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t c = static_cast<uint64_t>(blockIdx.x) * kDotWarps + warp;
     const uint64_t b = c * kChunk;
-    if (b >= N) return;
-    const uint64_t e = N - b < kChunk ? N : b + kChunk;
-    double s = 0.0;
-    for (uint64_t i = b; i < e; ++i) {
-        const double w = W[i];
-        s = __dadd_rn(s, __dmul_rn(w, w));
+    if (b >= N) return;  // warp-uniform; no CTA barrier below
+    const unsigned len = static_cast<unsigned>(N - b < kChunk ? N - b : kChunk);
+    for (unsigned i = lane; i < len; i += 32) {
+        const double w = W[b + i];
+        sq[warp][i] = __dmul_rn(w, w);
     }
-    dots[c] = s;
+    __syncwarp();
+    if (lane == 0) {
+        double s = 0.0;
+        for (unsigned i = 0; i < len; ++i) s = __dadd_rn(s, sq[warp][i]);
+        dots[c] = s;
+    }
 }
 
-__global__ void k_weight_finish(uint64_t nchunks, const double *dots, const double *accw, const long long *lmax_bits,
-    double *out /* [ess, log_nc, accw, lmax] */)
+// the chunk dots are added in order by thread 0 from shared memory, which
+// the CTA fills a tile at a time with coalesced loads
+constexpr int kFinishThreads = 256, kFinishTile = 2048;
+
+__global__ void __launch_bounds__(kFinishThreads) k_weight_finish(uint64_t nchunks, const double *dots,
+    const double *accw, const long long *lmax_bits, double *out /* [ess, log_nc, accw, lmax] */)
 {
-    if (threadIdx.x != 0) return;
+    __shared__ double tile[kFinishTile];
     double essw = 0.0;
-    for (uint64_t c = 0; c < nchunks; ++c) essw = __dadd_rn(essw, dots[c]);
+    for (uint64_t t0 = 0; t0 < nchunks; t0 += kFinishTile) {
+        const unsigned len = static_cast<unsigned>(nchunks - t0 < kFinishTile ? nchunks - t0 : kFinishTile);
+        for (unsigned i = threadIdx.x; i < len; i += kFinishThreads) tile[i] = dots[t0 + i];
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (unsigned i = 0; i < len; ++i) essw = __dadd_rn(essw, tile[i]);
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
     const double a = *accw;
     const double lmax = from_ordered_bits(*lmax_bits);
     out[0] = __ddiv_rn(__dmul_rn(a, a), essw);
@@ -120,11 +142,12 @@ int weight_normalize_dev(uint64_t N, double *W, const double *v, int add_log, vo
     MB_LAUNCH_CHECK();
     k_weight_exp<<<grid_cap(N, 256), 256, 0, s>>>(N, W, lmax_bits);
     MB_LAUNCH_CHECK();
-    k_weight_chunkdot<<<static_cast<unsigned>((nchunks + 127) / 128), 128, 0, s>>>(N, W, dots);
+    k_weight_chunkdot<<<static_cast<unsigned>((nchunks + kDotWarps - 1) / kDotWarps), 32 * kDotWarps, 0, s>>>(N, W,
+        dots);
     MB_LAUNCH_CHECK();
     int rc = fold_exact(W, N, 0.0, nullptr, fs, s);
     if (rc != MCKL_B200_OK) return rc;
-    k_weight_finish<<<1, 32, 0, s>>>(nchunks, dots, fs.final_v, lmax_bits, result_dev);
+    k_weight_finish<<<1, kFinishThreads, 0, s>>>(nchunks, dots, fs.final_v, lmax_bits, result_dev);
     MB_LAUNCH_CHECK();
     k_weight_scale<<<grid_cap(N, 256), 256, 0, s>>>(N, W, fs.final_v);
     MB_LAUNCH_CHECK();
