@@ -204,34 +204,39 @@ __global__ void __launch_bounds__(kWalkThreads) k_fold_walk(const double *x, uin
     __syncthreads();
     while (true) {
         if (warp == 0) {
-            // certain tiles: every lane tracks the same running value
+            // certain tiles, 32 at a time: lane l takes tile t + l; inside a
+            // run of certain tiles of the running sum's binade the entry
+            // counts are K + (exclusive prefix of the tiles' A), and the run
+            // ends at the first tile that is flagged, of another binade, or
+            // would leave the binade (then the CTA folds it exactly)
             double s = sh_s;
             uint64_t t = sh_t;
-            bool stop = false;
-            while (!stop && t < T) {
+            while (t < T) {
                 const uint64_t mine = t + lane;
                 FoldDesc d{0, 1, 0};
                 if (mine < T) d = desc[mine];
-                double my_start = 0.0;
-                int taken = 0;
-                for (int k = 0; k < 32 && t + k < T; ++k) {
-                    const int eb = __shfl_sync(0xffffffffu, d.eb, k);
-                    const int fl = __shfl_sync(0xffffffffu, d.flags, k);
-                    const long long A = __shfl_sync(0xffffffffu, d.A, k);
-                    const long long K = grid_count(s);
-                    if (fl || !(s > 0.0) || biased_exp(s) != eb || K + A >= grid_top(eb)) {
-                        stop = true;
-                        break;
-                    }
-                    if (lane == k) my_start = s;
-                    s = from_grid(K + A, eb);
-                    ++taken;
+                const int eb = biased_exp(s);
+                const long long K = grid_count(s);
+                // inclusive prefix of A over the lanes (unsigned: past the
+                // first tile that ends the run the sums are not used)
+                unsigned long long P = static_cast<unsigned long long>(d.A);
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const unsigned long long n = __shfl_up_sync(0xffffffffu, P, o);
+                    if (lane >= o) P += n;
                 }
+                const bool ok = s > 0.0 && !d.flags && d.eb == eb && d.A >= 0 &&
+                                P < static_cast<unsigned long long>(grid_top(eb) - K);
+                const unsigned bad = __ballot_sync(0xffffffffu, !ok);
+                const int taken = bad ? __ffs(bad) - 1 : 32;
                 if (lane < taken) {
-                    tstart[t + lane] = my_start;
-                    tmode[t + lane] = 0;
+                    tstart[mine] = from_grid(K + static_cast<long long>(P) - d.A, eb);
+                    tmode[mine] = 0;
                 }
+                if (taken == 0) break;
+                s = from_grid(K + static_cast<long long>(__shfl_sync(0xffffffffu, P, taken - 1)), eb);
                 t += taken;
+                if (taken < 32) break;
             }
             if (lane == 0) {
                 sh_s = s;
