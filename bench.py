@@ -445,7 +445,7 @@ def cpu_callers_reference():
             "sample": "N = 2^16, R = 100 random parents, column-major"}
 
 
-def bench_adjoint(rank, dev, sets=256, N=1 << 16, T=1000, C=32, threads=512):
+def bench_adjoint(rank, dev, sets=256, N=1 << 16, T=1000, C=32, threads=1024):
     """Differentiated SMC: gradient of the FP64 estimate in (phi, sx, sy) for
     `sets` parameter sets drawn like the batched workload, N particles, T
     observations, ancestors fixed and replayed from the counters."""
