@@ -26,8 +26,9 @@ class PFLogLikelihood(torch.autograd.Function):
         b = BatchedFilters(w["N"], w["y"], w["phi"], w["sx"], w["sy"], w["mkeys"], w["rkeys"],
                            threshold=w.get("threshold", 0.5), fp64=True)
         try:
-            if "threads" in w:
-                b.config(int(w["threads"]), int(w.get("ctas_per_sm", 1)))
+            # the adjoint kernel is fastest with 1024 threads per filter (twice
+            # the resident warps of 512, whatever it spills) unless told otherwise
+            b.config(int(w.get("threads", 1024)), int(w.get("ctas_per_sm", 1)))
             ll, g = b.adjoint(checkpoint_every)
         finally:
             b.close()
