@@ -63,6 +63,20 @@ const char *mckl_b200_version(void);
 /* Number of kernels this library has launched in this process (diagnostics;
  * no counterpart in the reference). */
 uint64_t mckl_b200_launch_count(void);
+/* Working memory.  Calls that need device working memory beyond their
+ * arguments (Weight, fold, resampling, rep -> index, the plain filter, Gamma,
+ * the index matrix, the weighted estimate) take it from buffers the library
+ * keeps per (device, stream): calls on different streams or host threads
+ * never share them, calls on one stream are ordered by it.  A buffer grows
+ * (stream-ordered, without synchronising the device) when a call needs more
+ * than the stream's previous calls; growing is refused with
+ * MCKL_B200_ERR_NOMEM while the stream is being captured into a CUDA graph,
+ * so make one call of the largest size on a stream before capturing it.
+ * mckl_b200_release_stream frees the buffers held for `stream` on the current
+ * device (after its queued work); call it before destroying a stream the
+ * library has used.  No counterpart in the reference (its objects own their
+ * buffers). */
+int mckl_b200_release_stream(void *stream);
 
 /* ---- engines (host-only state operations, no GPU work) ------------------ */
 

@@ -138,8 +138,12 @@ inline size_t align256(size_t n)
     return (n + 255) & ~static_cast<size_t>(255);
 }
 
-// Scratch device memory owned by the library, one growable buffer per device
-// and slot; reused across calls on the same stream order.
+// Working device memory owned by the library: one growable buffer per
+// (device, stream, slot), so calls on different streams never share it.
+// Returns nullptr when it cannot be obtained (or would have to grow while
+// the stream is being captured).
 void *scratch(int slot, size_t bytes, cudaStream_t stream);
+// Release the buffers of `stream` on the current device.
+int scratch_release(cudaStream_t stream);
 
 }  // namespace mckl_b200

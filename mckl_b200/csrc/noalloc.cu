@@ -14,7 +14,11 @@
 // The array below is a host-side symbol: code on the host must not pass its
 // name to a kernel (that would hand the GPU a host address).  The device
 // address is looked up with cudaGetSymbolAddress once per device, with that
-// device current, on the first call made on it, and cached.
+// device current, on the first call made on it, and cached; that first call
+// should therefore come before any stream capture.  The cached address
+// belongs to the device's primary context: after cudaDeviceReset on a device
+// the library's module is loaded again at a new address, so this entry point
+// must not be called on that device after a reset in the same process.
 #include <mutex>
 
 #include "common.cuh"
@@ -44,6 +48,11 @@ int static_scratch(void **out)
     MB_CHECK_ARG(dev >= 0 && dev < kMaxDevices, "device ordinal out of range");
     std::lock_guard<std::mutex> lk(g_static_mu);
     if (g_static_ptr[dev] == nullptr) {
+        // the fixed array must hold the working memory of the largest
+        // accepted call plus the results (the sizes come from the
+        // normaliser's own layout, so a change there is caught here)
+        MB_CHECK_ARG(weight_scratch_bytes(kStaticMaxN) + 256 <= kStaticScratchBytes,
+            "internal: the fixed working memory is smaller than the largest accepted call needs");
         void *p = nullptr;
         MB_CUDA(cudaGetSymbolAddress(&p, g_weight_scratch));
         g_static_ptr[dev] = p;
@@ -75,8 +84,8 @@ extern "C" int mckl_b200_weight_add_log_static(size_t N, double *W, const double
     cudaStream_t s = as_stream(stream);
     double *res = reinterpret_cast<double *>(static_cast<char *>(base) + weight_scratch_bytes(N));
     // every value the normaliser reads from its working memory is written
-    // first in the same call (the running maximum is reset by a copy), so the
-    // previous call's leftovers never leak into this one
+    // first in the same call (the running maximum is reset by a one-thread
+    // kernel), so the previous call's leftovers never leak into this one
     rc = weight_normalize_dev(N, W, v, 1, base, res, s);
     if (rc != MCKL_B200_OK) return rc;
     if (ess || log_nc_inc) {

@@ -16,7 +16,8 @@
 #include <type_traits>
 #include <cstring>
 #include <mutex>
-#include <unordered_map>
+#include <functional>
+#include <map>
 
 #include "common.cuh"
 #include "dispatch.cuh"
@@ -45,33 +46,72 @@ struct ScratchBuf {
     size_t bytes = 0;
 };
 
-static std::mutex g_scratch_mu;
-static std::unordered_map<long long, ScratchBuf> g_scratch;
+struct ScratchKey {
+    int dev;
+    cudaStream_t stream;
+    int slot;
+    bool operator<(const ScratchKey &o) const
+    {
+        if (dev != o.dev) return dev < o.dev;
+        if (stream != o.stream) return std::less<cudaStream_t>()(stream, o.stream);
+        return slot < o.slot;
+    }
+};
 
+static std::mutex g_scratch_mu;
+static std::map<ScratchKey, ScratchBuf> g_scratch;
+
+// One buffer per (device, stream, slot): calls on different streams never
+// share working memory, and calls on one stream are ordered by the stream.
+// The buffers come from the stream-ordered allocator, so a buffer that must
+// grow is released after the work already queued on its stream
+// (cudaFreeAsync) and replaced on the same stream without synchronising the
+// device.  Growing is refused while the stream is being captured (the
+// allocation would belong to the graph).
 void *scratch(int slot, size_t bytes, cudaStream_t stream)
 {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
-    const long long k = static_cast<long long>(dev) * 64 + slot;
     std::lock_guard<std::mutex> lk(g_scratch_mu);
-    ScratchBuf &b = g_scratch[k];
+    ScratchBuf &b = g_scratch[ScratchKey{dev, stream, slot}];
     if (b.bytes < bytes) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+            set_error("working memory must grow during stream capture; make one call of this size on the "
+                      "stream before capturing it");
+            return nullptr;
+        }
         if (b.ptr) {
-            // another stream might still use the old buffer: drain the device
-            if (cudaDeviceSynchronize() != cudaSuccess) return nullptr;
-            cudaFree(b.ptr);
+            if (cudaFreeAsync(b.ptr, stream) != cudaSuccess) return nullptr;
             b.ptr = nullptr;
             b.bytes = 0;
         }
-        size_t want = std::max<size_t>(bytes, 1 << 20);
-        if (cudaMalloc(&b.ptr, want) != cudaSuccess) {
+        const size_t want = std::max<size_t>(bytes, 1 << 20);
+        if (cudaMallocAsync(&b.ptr, want, stream) != cudaSuccess) {
             b.ptr = nullptr;
             return nullptr;
         }
         b.bytes = want;
     }
-    (void) stream;
     return b.ptr;
+}
+
+// Release every working buffer this library holds for `stream` on the
+// current device (after the work queued on it).
+int scratch_release(cudaStream_t stream)
+{
+    int dev = 0;
+    MB_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    for (auto it = g_scratch.begin(); it != g_scratch.end();) {
+        if (it->first.dev == dev && it->first.stream == stream) {
+            if (it->second.ptr) MB_CUDA(cudaFreeAsync(it->second.ptr, stream));
+            it = g_scratch.erase(it);
+        } else {
+            ++it;
+        }
+    }
+    return MCKL_B200_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -578,7 +618,12 @@ uint64_t mckl_b200_launch_count(void)
 
 const char *mckl_b200_version(void)
 {
-    return "mckl_b200 0.1 (sm_100a)";
+    return "mckl_b200 0.2 (sm_100a)";
+}
+
+int mckl_b200_release_stream(void *stream)
+{
+    return scratch_release(as_stream(stream));
 }
 
 int mckl_b200_engine_seed(mckl_b200_engine_t *e, uint32_t kind, uint64_t seed)

@@ -105,6 +105,11 @@ __global__ void __launch_bounds__(kFinishThreads) k_weight_finish(uint64_t nchun
     out[3] = lmax;
 }
 
+__global__ void k_weight_reset(long long *lmax_bits, long long v)
+{
+    *lmax_bits = v;
+}
+
 __global__ void k_weight_scale(uint64_t N, double *W, const double *accw)
 {
     const double inv = __ddiv_rn(1.0, *accw);
@@ -136,8 +141,10 @@ int weight_normalize_dev(uint64_t N, double *W, const double *v, int add_log, vo
     const uint64_t nchunks = (N + kChunk - 1) / kChunk;
     double *dots = reinterpret_cast<double *>(p + 256);
     FoldScratch fs = fold_scratch_carve(p + 256 + align256(nchunks * sizeof(double)), N);
-    const long long neg_inf = ordered_bits(-__builtin_huge_val());
-    MB_CUDA(cudaMemcpyAsync(lmax_bits, &neg_inf, sizeof(neg_inf), cudaMemcpyHostToDevice, s));
+    // the running maximum starts at -inf (a kernel, not a host copy: nothing
+    // here reads host memory, so the sequence can be captured in a graph)
+    k_weight_reset<<<1, 1, 0, s>>>(lmax_bits, ordered_bits(-__builtin_huge_val()));
+    MB_LAUNCH_CHECK();
     k_weight_prep<<<grid_cap(N, 256), 256, 0, s>>>(N, W, v, add_log, lmax_bits);
     MB_LAUNCH_CHECK();
     k_weight_exp<<<grid_cap(N, 256), 256, 0, s>>>(N, W, lmax_bits);

@@ -26,7 +26,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmckl_ref.so")
 REF_GENERIC_SO = os.path.join(HERE, "_ref", "libmckl_ref_generic.so")
-REF_ROOT = "/root/reference"
+# The reference's source tree: $MCKL_REF_ROOT, else a `reference` directory
+# beside this repository's root.
+REF_ROOT = os.environ.get("MCKL_REF_ROOT", os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 
 PHILOX4X32, PHILOX4X32_64, THREEFRY4X64, THREEFRY4X64_64, ARS, ARS_64 = range(1, 7)
 WORDS_PER_BLOCK = {1: 4, 2: 2, 3: 8, 4: 4, 5: 4, 6: 2}
@@ -116,9 +118,11 @@ class CPUPath:
             f("math_f64", [i, sz, vp, vp, vp])
             f("fold", [sz, vp, d, vp, vp])
             f("weighted_estimate", [sz, sz, i, vp, vp, vp])
+            f("gamma_blocks_from", [ep, i, sz, sz, sz, vp, d, vp, i])
         else:
             f("pf_ar1", [sz, sz, vp, d, d, d, d, vp, vp, i, d, i, vp, vp, vp, vp, vp, vp, i])
             f("pf_ar1_batch", [sz, vp, sz, vp, vp, vp, vp, vp, vp, i, d, vp, i])
+            f("pf_ar1_digest", [sz, sz, vp, d, d, d, d, vp, vp, i, d, vp, vp, vp, vp, vp])
             f("index_matrix", [sz, sz, vp, sz, sz, i, vp, vp])
             f("engine_to_text", [ep, ctypes.c_char_p, sz])
             f("engine_from_text", [ep, ctypes.c_char_p])
@@ -164,6 +168,14 @@ class CPUPath:
         out = np.zeros(len(alpha) * block, dtype=np.float64 if f64 else np.float32)
         assert self._gamma_blocks(ctypes.byref(eng), int(f64), len(alpha), block, _ptr(alpha), beta,
                                   _ptr(out), nthreads) == 0
+        return out
+
+    def gamma_blocks_from(self, eng, f64, first, block, alpha, beta=1.0, nthreads=1):
+        """Blocks first .. first + len(alpha) - 1 of gamma_blocks (oracle only)."""
+        alpha = np.ascontiguousarray(alpha, dtype=np.float64)
+        out = np.zeros(len(alpha) * block, dtype=np.float64 if f64 else np.float32)
+        assert self._gamma_blocks_from(ctypes.byref(eng), int(f64), first, len(alpha), block, _ptr(alpha), beta,
+                                       _ptr(out), nthreads) == 0
         return out
 
     # -- SMC ---------------------------------------------------------------
@@ -247,6 +259,23 @@ class CPUPath:
                          backend, _ptr(ll), _ptr(ess), _ptr(rs), _ptr(anc), _ptr(x), _ptr(W),
                          int(record))
         return dict(loglik=float(ll[0]), ess=ess, resampled=rs, anc=anc, x=x, W=W)
+
+    def pf_ar1_digest(self, N, y, phi, sx, sy, sd0, mkey, rkey, scheme=2, threshold=0.5):
+        """The reference's BackendSEQ filter with, per resampling iteration t,
+        two exact sums of its parent vector: digest[t] = (sum idx_i,
+        sum idx_i (i + 1)) (zeros where t did not resample)."""
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        T = len(y) - 1
+        mk = np.array(mkey, dtype=np.uint32)
+        rk = np.array(rkey, dtype=np.uint32)
+        ll = np.zeros(1)
+        ess = np.zeros(T + 1)
+        rs = np.zeros(T + 1, dtype=np.uint8)
+        dig = np.zeros((T + 1, 2), dtype=np.uint64)
+        x = np.zeros(N)
+        assert self._pf_ar1_digest(N, T, _ptr(y), phi, sx, sy, sd0, _ptr(mk), _ptr(rk), scheme, threshold,
+                                   _ptr(ll), _ptr(ess), _ptr(rs), _ptr(dig), _ptr(x)) == 0
+        return dict(loglik=float(ll[0]), ess=ess, resampled=rs, digest=dig, x=x)
 
     # -- oracle-only helpers ------------------------------------------------
     def simulate_ar1(self, T, phi, sx, sy, sd0, key):

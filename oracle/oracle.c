@@ -382,13 +382,21 @@ int orc_gamma(orc_engine *e, int is_f64, size_t n, void *r, double alpha, double
 int orc_gamma_blocks(const orc_engine *e, int is_f64, size_t nblocks, size_t block,
     const double *alpha, double beta, void *r, int nthreads)
 {
+    return orc_gamma_blocks_from(e, is_f64, 0, nblocks, block, alpha, beta, r, nthreads);
+}
+
+/* Blocks first .. first + nblocks - 1 of the same per-block form: block
+ * first + b is written to r + b * block, with shape alpha[b]. */
+int orc_gamma_blocks_from(const orc_engine *e, int is_f64, size_t first, size_t nblocks, size_t block,
+    const double *alpha, double beta, void *r, int nthreads)
+{
     (void) nthreads;
 #ifdef _OPENMP
 #pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads > 0 ? nthreads : 1)
 #endif
     for (long long b = 0; b < (long long) nblocks; ++b) {
         orc_engine s = *e;
-        s.ctr[0] = 0; s.ctr[1] = (uint64_t) b; s.ctr[2] = s.ctr[3] = 0;
+        s.ctr[0] = 0; s.ctr[1] = (uint64_t) (first + (size_t) b); s.ctr[2] = s.ctr[3] = 0;
         s.index = 0xFFFFFFFFu;
         if (is_f64) gamma_batch_f64(&s, block, (double *) r + (size_t) b * block, alpha[b], beta);
         else gamma_batch_f32(&s, block, (float *) r + (size_t) b * block, (float) alpha[b], (float) beta);

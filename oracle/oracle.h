@@ -40,6 +40,8 @@ int orc_exponential(orc_engine *e, int is_f64, size_t n, void *r, double lambda)
 int orc_gamma(orc_engine *e, int is_f64, size_t n, void *r, double alpha, double beta);
 int orc_gamma_blocks(const orc_engine *e, int is_f64, size_t nblocks, size_t block,
     const double *alpha, double beta, void *r, int nthreads);
+int orc_gamma_blocks_from(const orc_engine *e, int is_f64, size_t first, size_t nblocks, size_t block,
+    const double *alpha, double beta, void *r, int nthreads);
 
 int orc_weight_set_log(size_t N, const double *v, double *W, double *ess);
 int orc_weight_add_log(size_t N, double *W, const double *v, double *ess);

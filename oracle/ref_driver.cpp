@@ -25,6 +25,7 @@
 // block, the key, the Threefry tweak, and the number of words of that block
 // already handed out (index == words per block means nothing is buffered).
 
+#include <algorithm>
 #include <cstring>
 #include <mckl/algorithm/resample.hpp>
 #include <mckl/algorithm/smc.hpp>
@@ -649,7 +650,8 @@ template <typename Backend>
 int pf_run(std::size_t N, std::size_t T, const AR1Params &p,
     const std::uint32_t mkey[2], const std::uint32_t rkey[2], int scheme,
     double threshold, double *loglik, double *ess_hist, std::uint8_t *resampled,
-    std::uint64_t *anc, double *x_out, double *W_out, int record)
+    std::uint64_t *anc, double *x_out, double *W_out, int record,
+    std::uint64_t *digest = nullptr)
 {
     mckl::SMCSampler<AR1State> sampler(N);
     std::array<std::uint32_t, 2> mk = {{mkey[0], mkey[1]}};
@@ -689,6 +691,17 @@ int pf_run(std::size_t N, std::size_t T, const AR1Params &p,
                 for (std::size_t i = 0; i != n; ++i) {
                     anc[iter * n + i] = idx[i];
                 }
+            }
+            if (digest != nullptr) {
+                // two exact integer sums of the parent vector (no wrap below
+                // 2^31 particles): sum idx_i and sum idx_i (i + 1)
+                std::uint64_t d1 = 0, d2 = 0;
+                for (std::size_t i = 0; i != n; ++i) {
+                    d1 += idx[i];
+                    d2 += idx[i] * (i + 1);
+                }
+                digest[2 * iter] = d1;
+                digest[2 * iter + 1] = d2;
             }
             if (resampled != nullptr) {
                 resampled[iter] = 1;
@@ -751,6 +764,28 @@ int ref_pf_ar1(std::size_t N, std::size_t T, const double *y, double phi,
     }
     return pf_run<mckl::BackendSEQ>(N, T, p, mkey, rkey, scheme, threshold,
         loglik, ess_hist, resampled, anc, x_out, W_out, record);
+}
+
+// The same BackendSEQ run, recording per resampling iteration only two exact
+// sums of its parent vector (digest[2 t], digest[2 t + 1]; zero where the
+// iteration did not resample), so long runs at large N need no T x N record.
+int ref_pf_ar1_digest(std::size_t N, std::size_t T, const double *y,
+    double phi, double sx, double sy, double sd0, const std::uint32_t mkey[2],
+    const std::uint32_t rkey[2], int scheme, double threshold, double *loglik,
+    double *ess_hist, std::uint8_t *resampled, std::uint64_t *digest,
+    double *x_out)
+{
+    AR1Params p;
+    p.phi = phi;
+    p.sx = sx;
+    p.sy = sy;
+    p.sd0 = sd0;
+    p.y = y;
+    p.lconst = -std::log(sy) - 0.5 * std::log(2 * 3.14159265358979323846);
+    p.hinv = 0.5 / (sy * sy);
+    std::fill_n(digest, 2 * (T + 1), std::uint64_t(0));
+    return pf_run<mckl::BackendSEQ>(N, T, p, mkey, rkey, scheme, threshold,
+        loglik, ess_hist, resampled, nullptr, x_out, nullptr, 1, digest);
 }
 
 // Many independent filters (one BackendSEQ sampler each), OpenMP over filters.

@@ -8,7 +8,8 @@ with every ancestor vector.  Before writing, the seed-1 streams are checked
 against the reference's own known-answer files
 (example/random/random_<engine>[_64].data).
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # golden.npz
+    python tests/golden/make_golden.py --c3     # c3_full.npz (plain filter, N = 2^20, T = 1000)
 """
 import os
 import sys
@@ -94,5 +95,49 @@ def main():
     print("wrote", os.path.join(HERE, "golden.npz"), len(g), "arrays")
 
 
+C3_N, C3_T = 1 << 20, 1000
+
+
+def _c3_scheme(scheme):
+    """One scheme of the plain-filter configuration through the reference's
+    SMCSampler + BackendSEQ (a worker of make_c3)."""
+    ref = O.CPUPath("ref")
+    orc = O.CPUPath("oracle")
+    sd0 = 1 / np.sqrt(1 - 0.9 * 0.9)
+    _, y = orc.simulate_ar1(C3_T, 0.9, 1.0, 0.5, sd0, (7, 0))
+    res = ref.pf_ar1_digest(C3_N, y, 0.9, 1.0, 0.5, sd0, (11, 0), (12, 0), scheme)
+    x = res["x"]
+    return scheme, y, res["resampled"], res["digest"], res["loglik"], res["ess"], \
+        np.array([x.sum(), x.min(), x.max()])
+
+
+def make_c3():
+    """``c3_full.npz``: the plain-filter configuration (AR(1), phi 0.9, sx 1,
+    sy 0.5, T = 1000 observations simulated from seed 7, N = 2^20, model key
+    (11, 0), resampling key (12, 0), threshold 0.5) for the multinomial,
+    stratified, systematic and residual schemes: every iteration's resampling
+    decision, two exact sums of every parent vector (sum idx_i and
+    sum idx_i (i + 1)), the ESS history, the log-likelihood and the final
+    particles' sum / min / max.  About a minute per scheme on one core; the
+    four schemes run in parallel processes."""
+    import multiprocessing as mp
+
+    O.build(ref=True)
+    with mp.get_context("spawn").Pool(4) as pool:
+        out = pool.map(_c3_scheme, [0, 1, 2, 3])
+    g = {"y": out[0][1], "N": np.array([C3_N])}
+    for scheme, _, rs, dig, ll, ess, xs in out:
+        g[f"s{scheme}_resampled"] = rs
+        g[f"s{scheme}_digest"] = dig
+        g[f"s{scheme}_loglik"] = np.array([ll])
+        g[f"s{scheme}_ess"] = ess
+        g[f"s{scheme}_x"] = xs
+    np.savez_compressed(os.path.join(HERE, "c3_full.npz"), **g)
+    print("wrote", os.path.join(HERE, "c3_full.npz"), len(g), "arrays")
+
+
 if __name__ == "__main__":
-    main()
+    if "--c3" in sys.argv:
+        make_c3()
+    else:
+        main()

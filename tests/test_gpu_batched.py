@@ -17,6 +17,7 @@ import numpy as np
 import pytest
 
 torch = pytest.importorskip("torch")
+from conftest import require_cuda  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 import oracle as O  # noqa: E402
@@ -24,8 +25,7 @@ import oracle as O  # noqa: E402
 
 @pytest.fixture(scope="module")
 def env():
-    if not torch.cuda.is_available():
-        pytest.skip("no CUDA device")
+    require_cuda()
     import mckl_b200 as mb
 
     O.build()

@@ -15,6 +15,7 @@ import numpy as np
 import pytest
 
 torch = pytest.importorskip("torch")
+from conftest import require_cuda  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 import oracle as O  # noqa: E402
@@ -25,8 +26,7 @@ CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 
 @pytest.fixture(scope="module")
 def gpu():
-    if not torch.cuda.is_available():
-        pytest.skip("no CUDA device")
+    require_cuda()
 
 
 def test_reference_counter_engine_over_b200_generators(gpu):

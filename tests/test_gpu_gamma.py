@@ -18,6 +18,7 @@ import numpy as np
 import pytest
 
 torch = pytest.importorskip("torch")
+from conftest import require_cuda  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 import oracle as O  # noqa: E402
@@ -28,8 +29,7 @@ KINDS = {1: "Philox4x32", 2: "Philox4x32_64", 3: "Threefry4x64", 4: "Threefry4x6
 
 @pytest.fixture(scope="module")
 def env():
-    if not torch.cuda.is_available():
-        pytest.skip("no CUDA device")
+    require_cuda()
     import mckl_b200 as mb
 
     O.build()

@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 torch = pytest.importorskip("torch")
+from conftest import require_cuda  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 import oracle as O  # noqa: E402
@@ -14,8 +15,7 @@ import oracle as O  # noqa: E402
 
 @pytest.fixture(scope="module")
 def env():
-    if not torch.cuda.is_available():
-        pytest.skip("no CUDA device")
+    require_cuda()
     if not O.have_ref():
         pytest.skip("reference build missing")
     import mckl_b200 as mb

@@ -16,13 +16,13 @@ import numpy as np
 import pytest
 
 torch = pytest.importorskip("torch")
+from conftest import require_cuda  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 
 @pytest.fixture(scope="module")
 def lib():
-    if not torch.cuda.is_available():
-        pytest.skip("no CUDA device")
+    require_cuda()
     import mckl_b200 as mb
 
     L = mb.raw_lib()
@@ -45,7 +45,9 @@ def run(fn, W0, v):
 
 def test_static_matches_allocating_entry_point(lib):
     rng = np.random.default_rng(2024)
-    for N in (5000, 1 << 20):  # the same array serves both sizes, one after the other
+    # the same array serves every size, one after the other; 1 << 22 is the
+    # documented maximum, where the working memory nearly fills the array
+    for N in (5000, 1 << 20, 1 << 22):
         W0 = rng.random(N)
         W0 /= W0.sum()
         W0 = torch.from_numpy(W0).cuda()
