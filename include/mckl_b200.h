@@ -205,7 +205,7 @@ int mckl_b200_pf_ar1_plain_f64(size_t N, size_t T, const double *y, double phi, 
  * host programs that cannot let a library call cudaMalloc: plugins whose host
  * owns all device memory through its own pool or budget, code that must not
  * synchronize the device the way an allocation can, or processes running at
- * the memory limit.  Its working memory is a fixed 96 KiB array compiled into
+ * the memory limit.  Its working memory is a fixed 128 KiB array compiled into
  * the library, held on every GPU that loads it until the process exits; N is
  * limited to 4194304 (2^22) particles and larger N is rejected with
  * MCKL_B200_ERR_ARG.  The first call on a device looks up that array's device

@@ -76,6 +76,35 @@ __device__ __forceinline__ T block_inclusive_sum_1b(T v, T *sh, T *total)
     return warp > 0 ? before + inc : inc;
 }
 
+// Exclusive prefix sum over the CTA formed without a subtraction: each
+// thread's result is a sum of the values of the threads before it only, so
+// for floating-point inputs its rounding error is relative to itself (an
+// inclusive sum minus the own value would carry the error of the larger
+// inclusive sum).  `sh` needs 33 elements; the CTA total goes to *total.
+template <typename T>
+__device__ __forceinline__ T block_exclusive_sum(T v, T *sh, T *total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const T inc = warp_inclusive_sum(v);
+    T prev = __shfl_up_sync(0xffffffffu, inc, 1);
+    if (lane == 0) prev = T(0);
+    if (lane == 31) sh[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const T w = lane < nw ? sh[lane] : T(0);
+        const T wi = warp_inclusive_sum(w);
+        T we = __shfl_up_sync(0xffffffffu, wi, 1);
+        if (lane == 0) we = T(0);
+        if (lane < nw) sh[lane] = we;
+        if (lane == nw - 1) sh[32] = wi;
+    }
+    __syncthreads();
+    const T r = warp > 0 ? sh[warp] + prev : prev;
+    *total = sh[32];
+    __syncthreads();
+    return r;
+}
+
 template <typename T>
 __device__ __forceinline__ T block_sum(T v, T *sh)
 {

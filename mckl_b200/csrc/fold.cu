@@ -21,6 +21,81 @@ __device__ __forceinline__ double ulp_of(double v)
     return grid_unit(eb);
 }
 
+
+// ---------------------------------------------------------------------------
+// Approximate partial sums and the classification of every element.
+//
+// A_j is a parallel (tree) sum of s0 + x_0 + ... + x_j; S_j the sequential
+// fold.  Both are sums of nonnegative terms, so |A_j - S_j| <= (j + 1 + D)
+// 2^-53 A_j (first order) with D the depth of A's summation tree (below
+// 100 + T / 1024 here: 16 sequential adds per thread, two CTA scans, the
+// tile scan with its carries).  ulp(A) > 2^-53 A, so a margin of
+// 2 (j + 1) + 2 T + 160 ulps of A_j holds S_j with room to spare: when
+// [A_j - margin, A_j + margin] lies inside one binade, S_j certainly does.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int certain_binade(double A, uint64_t j, uint64_t T)
+{
+    const double m = (2.0 * static_cast<double>(j + 1) + 2.0 * static_cast<double>(T) + 160.0) * ulp_of(A);
+    const double lo = __dsub_rn(A, m), hi = __dadd_rn(A, m);
+    if (!(lo > 0.0)) return -1;
+    const int e = biased_exp(lo);
+    if (e == 0x7ff || biased_exp(hi) != e) return -1;
+    return e;
+}
+
+// The tile's kPer elements of this thread (zeros past n) and the
+// approximate partial sum before the first of them.
+__device__ __forceinline__ void tile_load(const double *x, uint64_t n, double s0, const double *tpre, uint64_t t,
+    double (&xv)[kPer], double *sh, double *Abefore)
+{
+    const uint64_t i0 = t * kFoldTile + static_cast<uint64_t>(threadIdx.x) * kPer;
+    double own = 0.0;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        xv[k] = i0 + k < n ? x[i0 + k] : 0.0;
+        own = __dadd_rn(own, xv[k]);
+    }
+    double tot;
+    const double ex = block_exclusive_sum(own, sh, &tot);
+    *Abefore = __dadd_rn(__dadd_rn(s0, tpre[t]), ex);
+}
+
+// Element j = i0 + k is a RUN element when the binades of S_{j-1} and S_j
+// are certain and equal and x_j's grid increment at that binade has no event
+// (tie, too large): then S_j = S_{j-1} + u q_j exactly.  Every other element
+// is a WINDOW: the walk folds it with a real double add.  Returns, per
+// element, q (0 for windows), the window bit and the certain binade of
+// S_{j-1} (-1: uncertain).
+__device__ __forceinline__ void classify(const double (&xv)[kPer], uint64_t i0, uint64_t n, uint64_t T, double s0,
+    double Abefore, long long (&q)[kPer], unsigned &win, int (&eprev)[kPer])
+{
+    int ep;
+    if (i0 == 0) {
+        ep = (s0 > 0.0 && biased_exp(s0) != 0x7ff) ? biased_exp(s0) : -1;  // s0 itself is exact
+    } else {
+        ep = certain_binade(Abefore, i0 - 1, T);
+    }
+    double A = Abefore;
+    win = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        const uint64_t j = i0 + k;
+        q[k] = 0;
+        eprev[k] = ep;
+        if (j < n) {
+            A = __dadd_rn(A, xv[k]);
+            const int ej = certain_binade(A, j, T);
+            bool ev = true;
+            if (ej >= 0 && ej == ep) q[k] = grid_increment(xv[k], ej, ev);
+            if (ev) {
+                q[k] = 0;
+                win |= 1u << k;
+            }
+            ep = ej;
+        }
+    }
+}
+
 // 1. approximate tile sums
 __global__ void __launch_bounds__(kDescThreads) k_fold_tilesum(const double *x, uint64_t n, double *tsum)
 {
@@ -35,7 +110,7 @@ __global__ void __launch_bounds__(kDescThreads) k_fold_tilesum(const double *x, 
     if (threadIdx.x == 0) tsum[blockIdx.x] = acc;
 }
 
-// 2. exclusive prefix of tile sums (one CTA)
+// 2. exclusive prefix of the tile sums (one CTA), formed without subtraction
 __global__ void __launch_bounds__(1024) k_fold_scan_tiles(const double *tsum, uint64_t T, double *tpre)
 {
     __shared__ double sh[33];
@@ -44,24 +119,42 @@ __global__ void __launch_bounds__(1024) k_fold_scan_tiles(const double *tsum, ui
         const uint64_t t = b + threadIdx.x;
         const double v = t < T ? tsum[t] : 0.0;
         double tot;
-        const double inc = block_inclusive_sum(v, sh, &tot);
-        if (t < T) tpre[t] = carry + (inc - v);
+        const double ex = block_exclusive_sum(v, sh, &tot);
+        if (t < T) tpre[t] = b == 0 ? ex : carry + ex;
         carry += tot;
     }
 }
 
-// 3. tile descriptors: binade certain for the whole tile, no event inside
-__global__ void __launch_bounds__(kDescThreads) k_fold_describe(const double *x, uint64_t n, double s0,
-    const double *tsum, const double *tpre, uint64_t T, FoldDesc *desc)
+// 3. per tile: the sum of the run increments and the number of windows; and
+// the tile descriptor of the event-loop walk (the fallback)
+__global__ void __launch_bounds__(kDescThreads) k_fold_count(const double *x, uint64_t n, double s0,
+    const double *tsum, const double *tpre, uint64_t T, long long *tq, unsigned *tw, FoldDesc *desc, int *elast)
 {
+    __shared__ double shd[33];
     __shared__ long long shl[33];
+    __shared__ unsigned shu[33];
     const uint64_t t = blockIdx.x;
     const uint64_t base = t * kFoldTile;
-    const double S = s0 + tpre[t];
-    const double hi_est = S + tsum[t];
-    // fold error after i additions is below i ulp(s_i) / 2; the tile-sum
-    // prefix adds its own few ulps: a generous bound
-    const double margin = static_cast<double>(2 * (base + kFoldTile) + 2 * T + 64) * ulp_of(hi_est);
+    const uint64_t i0 = base + static_cast<uint64_t>(threadIdx.x) * kPer;
+    double xv[kPer], Ab;
+    tile_load(x, n, s0, tpre, t, xv, shd, &Ab);
+    long long q[kPer];
+    unsigned win;
+    int ep[kPer];
+    classify(xv, i0, n, T, s0, Ab, q, win, ep);
+    long long qs = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) qs += q[k];
+    // the binade of the last element's run (the walk's tail check)
+    if (i0 <= n - 1 && n - 1 < i0 + kPer) {
+        const int k = static_cast<int>(n - 1 - i0);
+        *elast = (win >> k) & 1u ? -1 : ep[k];
+    }
+    // descriptor of the event-loop walk: the tile's binade, certain for the
+    // whole tile, and its increments at that binade
+    const double S = __dadd_rn(s0, tpre[t]);
+    const double hi_est = __dadd_rn(S, tsum[t]);
+    const double margin = static_cast<double>(2 * (base + kFoldTile) + 2 * T + 160) * ulp_of(hi_est);
     const double lo = S - margin, hi = hi_est + margin;
     int slow = !(lo > 0.0);
     const int eb = biased_exp(lo);
@@ -69,21 +162,93 @@ __global__ void __launch_bounds__(kDescThreads) k_fold_describe(const double *x,
     long long A = 0;
     int ev = 0;
     if (!slow) {
+#pragma unroll
         for (int k = 0; k < kPer; ++k) {
-            const uint64_t i = base + threadIdx.x * kPer + k;
-            if (i < n) {
+            if (i0 + k < n) {
                 bool e;
-                A += grid_increment(x[i], eb, e);
+                A += grid_increment(xv[k], eb, e);
                 ev |= e;
             }
         }
     }
     ev = __syncthreads_or(ev);
     A = block_sum(A, shl);
+    qs = block_sum(qs, shl);
+    const unsigned wc = block_sum(static_cast<unsigned>(__popc(win)), shu);
     if (threadIdx.x == 0) {
         desc[t].eb = eb;
         desc[t].flags = (slow || ev) ? 1 : 0;
         desc[t].A = A;
+        tq[t] = qs;
+        tw[t] = wc;
+    }
+}
+
+// 4. exclusive prefixes of the per-tile counts (one CTA); tot[0] = the sum of
+// all run increments, tot[1] = the number of windows
+__global__ void __launch_bounds__(1024) k_fold_scan_counts(const long long *tq, const unsigned *tw, uint64_t T,
+    long long *pq, unsigned long long *pw, long long *tot)
+{
+    __shared__ long long shl[33];
+    __shared__ unsigned long long shu[33];
+    long long cq = 0;
+    unsigned long long cw = 0;
+    for (uint64_t b = 0; b < T; b += blockDim.x) {
+        const uint64_t t = b + threadIdx.x;
+        const long long vq = t < T ? tq[t] : 0;
+        const unsigned long long vw = t < T ? tw[t] : 0;
+        long long totq;
+        unsigned long long totw;
+        const long long eq = block_exclusive_sum(vq, shl, &totq);
+        const unsigned long long ew = block_exclusive_sum(vw, shu, &totw);
+        if (t < T) {
+            pq[t] = cq + eq;
+            pw[t] = cw + ew;
+        }
+        cq += totq;
+        cw += totw;
+    }
+    if (threadIdx.x == 0) {
+        tot[0] = cq;
+        tot[1] = static_cast<long long>(cw);
+    }
+}
+
+// 5. the windows in order: index, value, run-increment prefix before it and
+// the binade of the run before it
+__global__ void __launch_bounds__(kDescThreads) k_fold_emit(const double *x, uint64_t n, double s0,
+    const double *tpre, uint64_t T, const long long *pq, const unsigned long long *pw, const long long *tot,
+    FoldWindows w)
+{
+    __shared__ double shd[33];
+    __shared__ long long shl[33];
+    __shared__ unsigned shu[33];
+    if (static_cast<unsigned long long>(tot[1]) > w.cap) return;  // the walk takes the event loop
+    const uint64_t t = blockIdx.x;
+    const uint64_t i0 = t * kFoldTile + static_cast<uint64_t>(threadIdx.x) * kPer;
+    double xv[kPer], Ab;
+    tile_load(x, n, s0, tpre, t, xv, shd, &Ab);
+    long long q[kPer];
+    unsigned win;
+    int ep[kPer];
+    classify(xv, i0, n, T, s0, Ab, q, win, ep);
+    long long qs = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) qs += q[k];
+    long long qtot;
+    unsigned wtot;
+    long long P = pq[t] + block_exclusive_sum(qs, shl, &qtot);
+    uint64_t r = pw[t] + block_exclusive_sum(static_cast<unsigned>(__popc(win)), shu, &wtot);
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        if ((win >> k) & 1u) {
+            w.idx[r] = i0 + k;
+            w.x[r] = xv[k];
+            w.P[r] = P;
+            w.e[r] = ep[k];
+            ++r;
+        }
+        P += q[k];
     }
 }
 
@@ -190,9 +355,12 @@ __device__ double fold_tile_exact(const double *x, uint64_t len, double s, doubl
     return s;
 }
 
-// 4. the walker: one CTA chains tile-entry values in order
-__global__ void __launch_bounds__(kWalkThreads) k_fold_walk(const double *x, uint64_t n, double s0,
-    const FoldDesc *desc, uint64_t T, double *tstart, int *tmode, double *prefix, double *final_v)
+// The event-loop walk (used when the windows do not fit their list, or if
+// the window walk ever met a value outside the binade it was classified in):
+// one CTA chains tile-entry values in order; certain tiles cost O(1), the
+// others are folded by the CTA with the event loop.
+__device__ void walk_events(const double *x, uint64_t n, double s0, const FoldDesc *desc, uint64_t T,
+    double *tstart, int *tmode, double *prefix, double *final_v)
 {
     __shared__ double sh_s;
     __shared__ unsigned long long sh_t;
@@ -262,12 +430,9 @@ __global__ void __launch_bounds__(kWalkThreads) k_fold_walk(const double *x, uin
     if (threadIdx.x == 0) *final_v = sh_s;
 }
 
-// 5. expand certain tiles to every partial sum
-__global__ void __launch_bounds__(kDescThreads) k_fold_expand(const double *x, uint64_t n, const FoldDesc *desc,
-    const double *tstart, const int *tmode, double *prefix)
+__device__ void expand_events(const double *x, uint64_t n, const FoldDesc *desc, const double *tstart,
+    const int *tmode, double *prefix, uint64_t t, long long *shl)
 {
-    __shared__ long long shl[33];
-    const uint64_t t = blockIdx.x;
     if (tmode[t] != 0) return;
     const uint64_t base = t * kFoldTile;
     const int eb = desc[t].eb;
@@ -291,56 +456,230 @@ __global__ void __launch_bounds__(kDescThreads) k_fold_expand(const double *x, u
     }
 }
 
-}  // namespace
+constexpr int kStage = 1024;  // window entries staged in shared memory per walk round
 
-size_t fold_scratch_bytes(uint64_t n)
+// 6. the walk (one CTA): the windows in order; the run before each window is
+// one integer step on its binade's grid, the window itself the reference's
+// own double add.  Writes the value after every window (mode 0).  When the
+// windows did not fit their list, or a run's value is not in the binade it
+// was classified in (the margins make that impossible; the check costs two
+// compares), the event-loop walk does the fold instead (mode 1).
+__global__ void __launch_bounds__(kWalkThreads) k_fold_walk(const double *x, uint64_t n, double s0,
+    const FoldDesc *desc, uint64_t T, double *tstart, int *tmode, double *prefix, double *final_v,
+    const long long *tot, const int *elast, FoldWindows w, int *mode)
 {
-    const uint64_t T = (n + kFoldTile - 1) / kFoldTile + 1;
-    return align256(T * sizeof(FoldDesc)) + 3 * align256(T * sizeof(double)) + align256(T * sizeof(int)) + 256;
+    __shared__ unsigned long long sj[kStage];
+    __shared__ double sx[kStage];
+    __shared__ long long sp[kStage];
+    __shared__ int se[kStage];
+    __shared__ int sh_ok;
+    __shared__ double sh_s;
+    __shared__ long long sh_p;
+    __shared__ unsigned long long sh_j;
+    const unsigned long long W = static_cast<unsigned long long>(tot[1]);
+    if (threadIdx.x == 0) {
+        sh_ok = W <= w.cap ? 1 : 0;
+        sh_s = s0;
+        sh_p = 0;
+        sh_j = 0;
+    }
+    __syncthreads();
+    for (unsigned long long c0 = 0; sh_ok && c0 < W; c0 += kStage) {
+        const unsigned m = static_cast<unsigned>(W - c0 < kStage ? W - c0 : kStage);
+        for (unsigned k = threadIdx.x; k < m; k += blockDim.x) {
+            sj[k] = w.idx[c0 + k];
+            sx[k] = w.x[c0 + k];
+            sp[k] = w.P[c0 + k];
+            se[k] = w.e[c0 + k];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double s = sh_s;
+            long long p = sh_p;
+            unsigned long long jn = sh_j;
+            int good = 1;
+            for (unsigned k = 0; k < m; ++k) {
+                if (sj[k] > jn) {  // the run jn .. sj[k] - 1
+                    const int e = se[k];
+                    if (!(s > 0.0) || biased_exp(s) != e) {
+                        good = 0;
+                        break;
+                    }
+                    const long long K = grid_count(s) + (sp[k] - p);
+                    if (K >= grid_top(e)) {
+                        good = 0;
+                        break;
+                    }
+                    s = from_grid(K, e);
+                }
+                s = __dadd_rn(s, sx[k]);
+                w.S[c0 + k] = s;
+                p = sp[k];
+                jn = sj[k] + 1;
+            }
+            sh_s = s;
+            sh_p = p;
+            sh_j = jn;
+            sh_ok = good;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && sh_ok) {
+        double s = sh_s;
+        if (sh_j < n) {  // the run after the last window
+            const int e = *elast;
+            const long long K = grid_count(s) + (tot[0] - sh_p);
+            if (e < 0 || !(s > 0.0) || biased_exp(s) != e || K >= grid_top(e)) {
+                sh_ok = 0;
+            } else {
+                s = from_grid(K, e);
+            }
+        }
+        if (sh_ok) {
+            *final_v = s;
+            *mode = 0;
+        }
+    }
+    __syncthreads();
+    if (!sh_ok) {
+        if (threadIdx.x == 0) *mode = 1;
+        walk_events(x, n, s0, desc, T, tstart, tmode, prefix, final_v);
+    }
 }
 
-FoldScratch fold_scratch_carve(void *base, uint64_t n)
+// 7. every partial sum, when the caller asks for them: a run element is the
+// value after the window before it plus its run's increments on the grid, a
+// window element the walk's value.
+__global__ void __launch_bounds__(kDescThreads) k_fold_expand(const double *x, uint64_t n, double s0,
+    const double *tpre, uint64_t T, const long long *pq, const unsigned long long *pw, FoldWindows w,
+    const int *mode, const FoldDesc *desc, const double *tstart, const int *tmode, double *prefix)
+{
+    __shared__ double shd[33];
+    __shared__ long long shl[33];
+    __shared__ unsigned shu[33];
+    const uint64_t t = blockIdx.x;
+    if (*mode != 0) {
+        expand_events(x, n, desc, tstart, tmode, prefix, t, shl);
+        return;
+    }
+    const uint64_t i0 = t * kFoldTile + static_cast<uint64_t>(threadIdx.x) * kPer;
+    double xv[kPer], Ab;
+    tile_load(x, n, s0, tpre, t, xv, shd, &Ab);
+    long long q[kPer];
+    unsigned win;
+    int ep[kPer];
+    classify(xv, i0, n, T, s0, Ab, q, win, ep);
+    long long qs = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) qs += q[k];
+    long long qtot;
+    unsigned wtot;
+    long long P = pq[t] + block_exclusive_sum(qs, shl, &qtot);
+    uint64_t r = pw[t] + block_exclusive_sum(static_cast<unsigned>(__popc(win)), shu, &wtot);
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        const uint64_t j = i0 + k;
+        if (j >= n) break;
+        if ((win >> k) & 1u) {
+            prefix[j] = w.S[r];
+            ++r;
+        } else {
+            P += q[k];
+            const double Sb = r > 0 ? w.S[r - 1] : s0;
+            const long long Pb = r > 0 ? w.P[r - 1] : 0;
+            prefix[j] = from_grid(grid_count(Sb) + (P - Pb), biased_exp(Sb));
+        }
+    }
+}
+
+__global__ void k_fold_set(double *v, double s0)
+{
+    *v = s0;
+}
+
+}  // namespace
+
+uint64_t fold_window_cap(uint64_t n)
+{
+    return std::min<uint64_t>(n + 1, 4096 + n / 256);
+}
+
+size_t fold_scratch_bytes(uint64_t n, uint64_t wcap)
 {
     const uint64_t T = (n + kFoldTile - 1) / kFoldTile + 1;
+    if (wcap == 0) wcap = fold_window_cap(n);
+    return align256(T * sizeof(FoldDesc)) + 3 * align256(T * sizeof(double)) + align256(T * sizeof(int)) +
+           align256(T * sizeof(long long)) + align256(T * sizeof(unsigned)) + align256(T * sizeof(long long)) +
+           align256(T * sizeof(unsigned long long)) + 256 + align256(wcap * sizeof(unsigned long long)) +
+           3 * align256(wcap * sizeof(double)) + align256(wcap * sizeof(int));
+}
+
+FoldScratch fold_scratch_carve(void *base, uint64_t n, uint64_t wcap)
+{
+    const uint64_t T = (n + kFoldTile - 1) / kFoldTile + 1;
+    if (wcap == 0) wcap = fold_window_cap(n);
     char *p = static_cast<char *>(base);
+    auto take = [&p](size_t bytes) {
+        char *q = p;
+        p += align256(bytes);
+        return q;
+    };
     FoldScratch f;
-    f.desc = reinterpret_cast<FoldDesc *>(p);
-    p += align256(T * sizeof(FoldDesc));
-    f.tsum = reinterpret_cast<double *>(p);
-    p += align256(T * sizeof(double));
-    f.tpre = reinterpret_cast<double *>(p);
-    p += align256(T * sizeof(double));
-    f.tstart = reinterpret_cast<double *>(p);
-    p += align256(T * sizeof(double));
-    f.tmode = reinterpret_cast<int *>(p);
-    p += align256(T * sizeof(int));
-    f.final_v = reinterpret_cast<double *>(p);
+    f.desc = reinterpret_cast<FoldDesc *>(take(T * sizeof(FoldDesc)));
+    f.tsum = reinterpret_cast<double *>(take(T * sizeof(double)));
+    f.tpre = reinterpret_cast<double *>(take(T * sizeof(double)));
+    f.tstart = reinterpret_cast<double *>(take(T * sizeof(double)));
+    f.tmode = reinterpret_cast<int *>(take(T * sizeof(int)));
+    f.tq = reinterpret_cast<long long *>(take(T * sizeof(long long)));
+    f.tw = reinterpret_cast<unsigned *>(take(T * sizeof(unsigned)));
+    f.pq = reinterpret_cast<long long *>(take(T * sizeof(long long)));
+    f.pw = reinterpret_cast<unsigned long long *>(take(T * sizeof(unsigned long long)));
+    char *small = take(256);
+    f.final_v = reinterpret_cast<double *>(small);
+    f.tot = reinterpret_cast<long long *>(small + 64);
+    f.elast = reinterpret_cast<int *>(small + 128);
+    f.mode = reinterpret_cast<int *>(small + 192);
+    f.win.idx = reinterpret_cast<unsigned long long *>(take(wcap * sizeof(unsigned long long)));
+    f.win.x = reinterpret_cast<double *>(take(wcap * sizeof(double)));
+    f.win.P = reinterpret_cast<long long *>(take(wcap * sizeof(long long)));
+    f.win.S = reinterpret_cast<double *>(take(wcap * sizeof(double)));
+    f.win.e = reinterpret_cast<int *>(take(wcap * sizeof(int)));
+    f.win.cap = wcap;
     return f;
 }
 
 int fold_exact(const double *x, uint64_t n, double s0, double *prefix, FoldScratch &fs, cudaStream_t s)
 {
     if (n == 0) {
-        MB_CUDA(cudaMemcpyAsync(fs.final_v, &s0, sizeof(double), cudaMemcpyHostToDevice, s));
+        k_fold_set<<<1, 1, 0, s>>>(fs.final_v, s0);
+        MB_LAUNCH_CHECK();
         return MCKL_B200_OK;
     }
     const uint64_t T = (n + kFoldTile - 1) / kFoldTile;
-    k_fold_tilesum<<<static_cast<unsigned>(T), kDescThreads, 0, s>>>(x, n, fs.tsum);
+    const unsigned nt = static_cast<unsigned>(T);
+    k_fold_tilesum<<<nt, kDescThreads, 0, s>>>(x, n, fs.tsum);
     MB_LAUNCH_CHECK();
     k_fold_scan_tiles<<<1, 1024, 0, s>>>(fs.tsum, T, fs.tpre);
     MB_LAUNCH_CHECK();
-    k_fold_describe<<<static_cast<unsigned>(T), kDescThreads, 0, s>>>(x, n, s0, fs.tsum, fs.tpre, T, fs.desc);
+    k_fold_count<<<nt, kDescThreads, 0, s>>>(x, n, s0, fs.tsum, fs.tpre, T, fs.tq, fs.tw, fs.desc, fs.elast);
     MB_LAUNCH_CHECK();
-    k_fold_walk<<<1, kWalkThreads, 0, s>>>(x, n, s0, fs.desc, T, fs.tstart, fs.tmode, prefix, fs.final_v);
+    k_fold_scan_counts<<<1, 1024, 0, s>>>(fs.tq, fs.tw, T, fs.pq, fs.pw, fs.tot);
+    MB_LAUNCH_CHECK();
+    k_fold_emit<<<nt, kDescThreads, 0, s>>>(x, n, s0, fs.tpre, T, fs.pq, fs.pw, fs.tot, fs.win);
+    MB_LAUNCH_CHECK();
+    k_fold_walk<<<1, kWalkThreads, 0, s>>>(x, n, s0, fs.desc, T, fs.tstart, fs.tmode, prefix, fs.final_v, fs.tot,
+        fs.elast, fs.win, fs.mode);
     MB_LAUNCH_CHECK();
     if (prefix) {
-        k_fold_expand<<<static_cast<unsigned>(T), kDescThreads, 0, s>>>(x, n, fs.desc, fs.tstart, fs.tmode, prefix);
+        k_fold_expand<<<nt, kDescThreads, 0, s>>>(x, n, s0, fs.tpre, T, fs.pq, fs.pw, fs.win, fs.mode, fs.desc,
+            fs.tstart, fs.tmode, prefix);
         MB_LAUNCH_CHECK();
     }
     return MCKL_B200_OK;
 }
 
 }  // namespace mckl_b200
+
 
 using namespace mckl_b200;
 

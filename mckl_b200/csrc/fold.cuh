@@ -19,16 +19,27 @@
 // At an event the single step is done with a real double add, which is the
 // reference's own operation.
 //
-// Parallel structure over tiles of kFoldTile elements:
-//   1. k_fold_tilesum / k_fold_scan_tiles: approximate tile sums and their
-//      prefix predict each tile's binade, with an error margin;
-//   2. k_fold_describe: tiles whose whole range is certainly inside one
-//      binade and holds no event get A_t = sum of q_i (a transfer function
-//      s -> s + u A_t);
-//   3. k_fold_walk (one CTA): chains the exact tile-entry values; certain
-//      tiles cost O(1), the others are folded by the CTA with the event loop;
-//   4. k_fold_expand: every element of the certain tiles gets
-//      s_i = s_entry + u * (prefix of q within the tile).
+// Parallel structure (tiles of kFoldTile elements):
+//   1. approximate partial sums A_j (a tree sum) carry a rigorous error bound,
+//      so for most elements the binade of the exact partial sum S_j is
+//      certain; an element whose S_{j-1} and S_j are certainly in the same
+//      binade, with an event-free increment, is a RUN element
+//      (S_j = S_{j-1} + u q_j); every other element -- a binade crossing, a
+//      tie, an uncertain binade -- is a WINDOW (typically a few dozen per
+//      fold: one per doubling of the sum);
+//   2. per tile, the run increments are summed and the windows counted; an
+//      exclusive scan over tiles places every window in an ordered list with
+//      the run-increment prefix before it;
+//   3. one thread walks the windows in order: the run before a window is a
+//      single integer step on its grid, the window the reference's own
+//      double add;
+//   4. every partial sum, when asked for, is the value after the window
+//      before it plus its run's increments.
+// When the windows do not fit their list (inputs with ties everywhere, long
+// zero or subnormal stretches) the walk falls back to the event loop: tiles
+// certain for their whole length cost O(1) (a transfer function s -> s +
+// u A_t), the others are folded by one CTA that handles one event per scan
+// round.
 #pragma once
 
 #include <cstdint>
@@ -109,20 +120,43 @@ __device__ __forceinline__ long long grid_increment(double x, int eb, bool &even
     return q;
 }
 
+// The windows of one fold, in order: element index, value, the sum of the run
+// increments of the elements before it, the binade of the run before it
+// (-1: none), and, after the walk, the fold's value after it.
+struct FoldWindows {
+    unsigned long long *idx;
+    double *x;
+    long long *P;
+    double *S;
+    int *e;
+    uint64_t cap;
+};
+
 struct FoldScratch {
     double *tsum;     // [T] approximate tile sums
     double *tpre;     // [T] approximate exclusive prefix of tile sums
-    FoldDesc *desc;   // [T]
-    double *tstart;   // [T] exact fold value entering each tile
-    int *tmode;       // [T] 0: expand from tstart, 1: values already written
+    FoldDesc *desc;   // [T] tile descriptors of the event-loop walk
+    double *tstart;   // [T] event-loop walk: exact value entering each tile
+    int *tmode;       // [T] event-loop walk: 0 expand from tstart, 1 values already written
+    long long *tq;    // [T] sum of the run increments of each tile
+    unsigned *tw;     // [T] windows in each tile
+    long long *pq;    // [T] exclusive prefix of tq
+    unsigned long long *pw;  // [T] exclusive prefix of tw
+    long long *tot;   // [2] all run increments, all windows
+    int *elast;       // binade of the run holding the last element (-1: it is a window)
+    int *mode;        // 0 window walk, 1 event-loop walk
     double *final_v;  // [1] the fold's last value
+    FoldWindows win;
 };
 
 // Host driver (fold.cu): folds x[0..n) starting from s0.  `prefix` (device,
 // nullable) receives every partial sum; the last one is also left in
-// scratch.final_v.  Returns an MCKL_B200_* status.
+// scratch.final_v.  Returns an MCKL_B200_* status.  `wcap`: capacity of the
+// window list (0: fold_window_cap(n)); a fold with more windows than that
+// takes the event-loop walk.
 int fold_exact(const double *x, uint64_t n, double s0, double *prefix, FoldScratch &fs, cudaStream_t s);
-size_t fold_scratch_bytes(uint64_t n);
-FoldScratch fold_scratch_carve(void *base, uint64_t n);
+uint64_t fold_window_cap(uint64_t n);
+size_t fold_scratch_bytes(uint64_t n, uint64_t wcap = 0);
+FoldScratch fold_scratch_carve(void *base, uint64_t n, uint64_t wcap = 0);
 
 }  // namespace mckl_b200

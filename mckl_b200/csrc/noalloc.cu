@@ -30,9 +30,13 @@ namespace {
 
 // Largest particle count the fixed working memory serves.
 constexpr uint64_t kStaticMaxN = 1ull << 22;
+// Window list of the exact sum in the fixed working memory: a sum of
+// normalised weights has a few dozen windows; one with more takes the exact
+// sum's event-loop path, which needs no list.
+constexpr uint64_t kStaticWindows = 256;
 // Bytes of fixed working memory per device: the normaliser's scratch for
 // kStaticMaxN particles plus 256 bytes of results, rounded up.
-constexpr size_t kStaticScratchBytes = 96 * 1024;
+constexpr size_t kStaticScratchBytes = 128 * 1024;
 
 static __device__ __align__(256) unsigned char g_weight_scratch[kStaticScratchBytes];
 
@@ -51,7 +55,7 @@ int static_scratch(void **out)
         // the fixed array must hold the working memory of the largest
         // accepted call plus the results (the sizes come from the
         // normaliser's own layout, so a change there is caught here)
-        MB_CHECK_ARG(weight_scratch_bytes(kStaticMaxN) + 256 <= kStaticScratchBytes,
+        MB_CHECK_ARG(weight_scratch_bytes(kStaticMaxN, kStaticWindows) + 256 <= kStaticScratchBytes,
             "internal: the fixed working memory is smaller than the largest accepted call needs");
         void *p = nullptr;
         MB_CUDA(cudaGetSymbolAddress(&p, g_weight_scratch));
@@ -72,7 +76,7 @@ extern "C" int mckl_b200_weight_add_log_static(size_t N, double *W, const double
 {
     MB_CHECK_ARG(N > 0, "N must be positive");
     MB_CHECK_ARG(W != nullptr && v != nullptr, "null pointer");
-    if (N > kStaticMaxN || weight_scratch_bytes(N) + 256 > kStaticScratchBytes) {
+    if (N > kStaticMaxN || weight_scratch_bytes(N, kStaticWindows) + 256 > kStaticScratchBytes) {
         set_error("mckl_b200_weight_add_log_static: N = " + std::to_string(N) +
                   " exceeds the fixed working memory (at most " + std::to_string(kStaticMaxN) +
                   " particles); use mckl_b200_weight_add_log");
@@ -82,11 +86,11 @@ extern "C" int mckl_b200_weight_add_log_static(size_t N, double *W, const double
     int rc = static_scratch(&base);
     if (rc != MCKL_B200_OK) return rc;
     cudaStream_t s = as_stream(stream);
-    double *res = reinterpret_cast<double *>(static_cast<char *>(base) + weight_scratch_bytes(N));
+    double *res = reinterpret_cast<double *>(static_cast<char *>(base) + weight_scratch_bytes(N, kStaticWindows));
     // every value the normaliser reads from its working memory is written
     // first in the same call (the running maximum is reset by a one-thread
     // kernel), so the previous call's leftovers never leak into this one
-    rc = weight_normalize_dev(N, W, v, 1, base, res, s);
+    rc = weight_normalize_dev(N, W, v, 1, base, res, s, kStaticWindows);
     if (rc != MCKL_B200_OK) return rc;
     if (ess || log_nc_inc) {
         double h[2];

@@ -127,20 +127,20 @@ unsigned grid_cap(uint64_t n, int threads)
 
 }  // namespace
 
-size_t weight_scratch_bytes(uint64_t N)
+size_t weight_scratch_bytes(uint64_t N, uint64_t wcap)
 {
     const uint64_t nchunks = (N + kChunk - 1) / kChunk;
-    return 256 + align256(nchunks * sizeof(double)) + fold_scratch_bytes(N);
+    return 256 + align256(nchunks * sizeof(double)) + fold_scratch_bytes(N, wcap);
 }
 
 int weight_normalize_dev(uint64_t N, double *W, const double *v, int add_log, void *scratch_base,
-    double *result_dev, cudaStream_t s)
+    double *result_dev, cudaStream_t s, uint64_t wcap)
 {
     char *p = static_cast<char *>(scratch_base);
     long long *lmax_bits = reinterpret_cast<long long *>(p);
     const uint64_t nchunks = (N + kChunk - 1) / kChunk;
     double *dots = reinterpret_cast<double *>(p + 256);
-    FoldScratch fs = fold_scratch_carve(p + 256 + align256(nchunks * sizeof(double)), N);
+    FoldScratch fs = fold_scratch_carve(p + 256 + align256(nchunks * sizeof(double)), N, wcap);
     // the running maximum starts at -inf (a kernel, not a host copy: nothing
     // here reads host memory, so the sequence can be captured in a graph)
     k_weight_reset<<<1, 1, 0, s>>>(lmax_bits, ordered_bits(-__builtin_huge_val()));
