@@ -420,6 +420,10 @@ def bench_plain_c3(N=1 << 20, T=1000):
     return {"workload": f"plain FP64 particle filter, N = 2^20, T = {T}, systematic resampling at ESS < N/2",
             "particle_steps_per_s": N * T / dt, "s": round(dt, 3), "resampling_steps": int(res["resampled"].sum()),
             "loglik": res["loglik"], "loglik_minus_kalman": float(res["loglik"] - kf[0]),
+            "scan_ties": res["ties"],
+            "scan_ties_note": "uniforms within one representable step of a cumulative weight, over all resampling "
+                              "steps; the cumulative weights are the reference's sequential fold bit for bit, so "
+                              "a tie flips no ancestor",
             "bound": "host round trip per step (the reference's step order: normaliser and ESS read back)",
             "y": y}
 

@@ -200,6 +200,15 @@ int mckl_b200_pf_ar1_plain_f64(size_t N, size_t T, const double *y, double phi, 
     const uint32_t mkey[2], const uint32_t rkey[2], int scheme, double threshold, double *loglik,
     double *ess_hist, uint8_t *resampled, uint64_t *anc_dev, double *x_dev, double *W_dev, void *stream);
 
+/* Scan ties of the calling thread's last mckl_b200_pf_ar1_plain_f64 run: the
+ * number of (uniform, cumulative weight) pairs over all its resampling steps
+ * whose uniform lies within one representable step of the cumulative weight
+ * (prev(c_i) <= u_j <= next(c_i)).  Those are the only comparisons that a
+ * cumulative weight one ulp off would decide the other way; the cumulative
+ * weights here are the reference's sequential fold bit for bit, so a tie
+ * changes no ancestor.  Diagnostics; no counterpart in the reference. */
+int mckl_b200_pf_ar1_plain_ties(uint64_t *ties);
+
 /* Weight::add_log without any device allocation (no counterpart in the
  * reference).  Same contract and results as mckl_b200_weight_add_log, for
  * host programs that cannot let a library call cudaMalloc: plugins whose host

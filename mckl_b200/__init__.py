@@ -161,6 +161,7 @@ def select(idx, state):
 
 _pf_plain = _bind("mckl_b200_pf_ar1_plain_f64", [_sz, _sz, _vp, _d, _d, _d, _d, _vp, _vp, _i, _d, _vp, _vp,
                                                    _vp, _vp, _vp, _vp, _vp])
+_pf_plain_ties = _bind("mckl_b200_pf_ar1_plain_ties", [ctypes.POINTER(ctypes.c_uint64)])
 
 
 def pf_ar1_plain(N, y, phi, sx, sy, sd0, mkey, rkey, scheme=2, threshold=0.5, record=False):
@@ -181,7 +182,9 @@ def pf_ar1_plain(N, y, phi, sx, sy, sd0, mkey, rkey, scheme=2, threshold=0.5, re
                      rs.ctypes.data_as(ctypes.c_void_p),
                      ctypes.c_void_p(anc.data_ptr()) if anc is not None else None,
                      ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(W.data_ptr()), _stream_ptr()))
-    return dict(loglik=ll.value, ess=ess, resampled=rs, anc=anc, x=x, W=W)
+    ties = ctypes.c_uint64()
+    _check(_pf_plain_ties(ctypes.byref(ties)))
+    return dict(loglik=ll.value, ess=ess, resampled=rs, anc=anc, x=x, W=W, ties=int(ties.value))
 
 
 _bt_create = _bind("mckl_b200_batched_create", [_vp, _sz, _vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _d, _i])

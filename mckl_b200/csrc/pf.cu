@@ -49,6 +49,9 @@ unsigned grid_of(uint64_t n)
     return static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 148 * 16)));
 }
 
+// scan ties of the calling thread's last plain-filter run
+thread_local uint64_t g_last_ties = 0;
+
 }  // namespace
 
 }  // namespace mckl_b200
@@ -79,6 +82,7 @@ extern "C" int mckl_b200_pf_ar1_plain_f64(size_t N, size_t T, const double *y, d
     uint64_t *idx = reinterpret_cast<uint64_t *>(base + 3 * align256(N * 8));
     double *wres = reinterpret_cast<double *>(base + 4 * align256(N * 8));
     int *err = reinterpret_cast<int *>(base + 4 * align256(N * 8) + 256);
+    unsigned long long *ties = reinterpret_cast<unsigned long long *>(base + 4 * align256(N * 8) + 384);
     void *wscr = base + buf;
     void *rscr = base + buf + wsz;
     void *iscr = base + buf + wsz + rsz;
@@ -96,6 +100,7 @@ extern "C" int mckl_b200_pf_ar1_plain_f64(size_t N, size_t T, const double *y, d
     const double hinv = 0.5 / (sy * sy);
     const double equal = 1.0 / static_cast<double>(N);
     MB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+    MB_CUDA(cudaMemsetAsync(ties, 0, sizeof(unsigned long long), s));
     k_fill<<<grid_of(N), 256, 0, s>>>(N, W_dev, equal);
     MB_LAUNCH_CHECK();
     double ess = static_cast<double>(N), ll_sum = 0.0;
@@ -119,7 +124,7 @@ extern "C" int mckl_b200_pf_ar1_plain_f64(size_t N, size_t T, const double *y, d
         if (ess_hist) ess_hist[it] = ess;
         if (resampled) resampled[it] = 0;
         if (ess < static_cast<double>(N) * threshold) {
-            int rc = resample_dev(scheme, N, N, er, W_dev, rep, rscr, s);
+            int rc = resample_dev(scheme, N, N, er, W_dev, rep, rscr, s, ties);
             if (rc != MCKL_B200_OK) return rc;
             rc = rep_to_index_dev(N, N, rep, idx, iscr, err, s);
             if (rc != MCKL_B200_OK) return rc;
@@ -135,12 +140,22 @@ extern "C" int mckl_b200_pf_ar1_plain_f64(size_t N, size_t T, const double *y, d
         }
     }
     int h = 0;
+    unsigned long long nt = 0;
     MB_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MB_CUDA(cudaMemcpyAsync(&nt, ties, sizeof(nt), cudaMemcpyDeviceToHost, s));
     MB_CUDA(cudaStreamSynchronize(s));
     if (h) {
         set_error("particle filter: a look-back wait exceeded its limit");
         return MCKL_B200_ERR_DEVICE;
     }
+    g_last_ties = nt;
     *loglik = ll_sum;
+    return MCKL_B200_OK;
+}
+
+extern "C" int mckl_b200_pf_ar1_plain_ties(uint64_t *ties)
+{
+    MB_CHECK_ARG(ties != nullptr, "null argument");
+    *ties = g_last_ties;
     return MCKL_B200_OK;
 }

@@ -113,14 +113,39 @@ __device__ __forceinline__ uint64_t lower_bound(const double *u, uint64_t M, dou
     return lo;
 }
 
-// rep_i from the cumulative weights c (length N - 1) and sorted uniforms u
-__global__ void k_rep_counts(uint64_t N, uint64_t M, const double *c, const double *u, uint64_t *rep)
+// the neighbouring doubles of v >= 0 (v below the largest finite double)
+__device__ __forceinline__ double next_up(double v)
 {
+    return __longlong_as_double(__double_as_longlong(v) + 1);
+}
+
+__device__ __forceinline__ double next_down(double v)
+{
+    return v > 0.0 ? __longlong_as_double(__double_as_longlong(v) - 1) : v;
+}
+
+// rep_i from the cumulative weights c (length N - 1) and sorted uniforms u.
+// With `ties` set, also counts the uniforms within one representable step of
+// a cumulative weight (prev(c_i) <= u_j <= next(c_i)): the comparisons
+// u_j < c_i that a cumulative weight one ulp off would decide the other way.
+__global__ void k_rep_counts(uint64_t N, uint64_t M, const double *c, const double *u, uint64_t *rep,
+    unsigned long long *ties)
+{
+    __shared__ unsigned long long sh[33];
+    unsigned long long nt = 0;
     GRID_LOOP(i, N)
     {
         const uint64_t prev = i == 0 ? 0 : lower_bound(u, M, c[i - 1]);
         const uint64_t cur = (i + 1 == N) ? M : lower_bound(u, M, c[i]);
         rep[i] = cur - prev;
+        if (ties && i + 1 < N) {
+            const double ci = c[i];
+            nt += lower_bound(u, M, next_up(next_up(ci))) - lower_bound(u, M, next_down(ci));
+        }
+    }
+    if (ties) {
+        nt = block_sum(nt, sh);
+        if (threadIdx.x == 0 && nt) atomicAdd(ties, nt);
     }
 }
 
@@ -379,7 +404,7 @@ int u01_sequence_dev(int kind, mckl_b200_engine_t &e, uint64_t n, double *u, dou
 }
 
 int resample_dev(int scheme, uint64_t N, uint64_t M, mckl_b200_engine_t &e, const double *W, uint64_t *rep,
-    void *scratch_base, cudaStream_t s)
+    void *scratch_base, cudaStream_t s, unsigned long long *ties_dev)
 {
     static const int seq_of[6] = {0, 1, 2, 0, 1, 2};
     const int seq = seq_of[scheme];
@@ -422,7 +447,7 @@ int resample_dev(int scheme, uint64_t N, uint64_t M, mckl_b200_engine_t &e, cons
     } else {
         rc = fold_exact(weights, N - 1, 0.0, tmp, fs, s);  // cumulative weights of particles 0..N-2
         if (rc != MCKL_B200_OK) return rc;
-        k_rep_counts<<<cap_grid(N, 256), 256, 0, s>>>(N, R, tmp, u, rep);
+        k_rep_counts<<<cap_grid(N, 256), 256, 0, s>>>(N, R, tmp, u, rep, ties_dev);
         MB_LAUNCH_CHECK();
     }
     if (scheme >= 3) {

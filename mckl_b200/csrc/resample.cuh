@@ -21,9 +21,11 @@ int u01_sequence_dev(int kind, mckl_b200_engine_t &e, uint64_t n, double *u, dou
 // ResampleAlgorithm::operator()(N, M, rng, W, rep); scheme 0 multinomial,
 // 1 stratified, 2 systematic, 3 residual, 4 residual-stratified,
 // 5 residual-systematic.  Residual schemes synchronize (the number of
-// uniforms they draw depends on the weights).
+// uniforms they draw depends on the weights).  ties_dev (device, nullable):
+// incremented by the number of uniforms within one representable step of a
+// cumulative weight.
 int resample_dev(int scheme, uint64_t N, uint64_t M, mckl_b200_engine_t &e, const double *W, uint64_t *rep,
-    void *scratch_base, cudaStream_t s);
+    void *scratch_base, cudaStream_t s, unsigned long long *ties_dev = nullptr);
 int rep_to_index_dev(uint64_t N, uint64_t M, const uint64_t *rep, uint64_t *idx, void *scratch_base, int *err_dev,
     cudaStream_t s);
 template <typename T>
