@@ -348,6 +348,24 @@ int mckl_b200_pmcmc_ar1(size_t C, const size_t *N, size_t T, const double *y, co
                         int fp64, double threshold, double *theta_out, double *loglik_out, uint32_t *accepted,
                         void *stream);
 
+/* The same chains with the proposal as a hook: PMCMCMutation's `update`
+ * evaluations (algorithm/pmcmc.hpp:116-145, the sum at :141-145), each of
+ * which takes the chain's RNG and a copy of the parameters, changes the copy
+ * and returns its log proposal ratio.  `proposal(c, i, words, theta, user)`
+ * is called for chain c at iteration i >= 1 with four Philox4x32 words
+ * (key (seed, c), counter 2i: the randomness the built-in random walk turns
+ * into its three normals) and theta = a copy of the chain's (phi, sx, sy) to
+ * change in place; it returns log q(theta | theta') - log q(theta' | theta)
+ * (0 for a symmetric proposal; a non-finite value rejects the proposal), which
+ * enters the acceptance sum where the reference adds its evaluations.
+ * mckl_b200_pmcmc_ar1 is this call with the Gaussian random walk. */
+typedef double (*mckl_b200_proposal_t)(size_t chain, size_t iter, const uint32_t words[4], double *theta,
+                                       void *user);
+int mckl_b200_pmcmc_ar1_proposal(size_t C, const size_t *N, size_t T, const double *y, const double *theta0,
+                                 mckl_b200_proposal_t proposal, void *proposal_user, mckl_b200_log_prior_t prior,
+                                 void *user, size_t iters, uint32_t seed, int fp64, double threshold,
+                                 double *theta_out, double *loglik_out, uint32_t *accepted, void *stream);
+
 /* ---- diagnostics (no counterpart in the reference) ----------------------
  * The library's double-double log (fn 0), exp (fn 1) and sin/cos (fn 2; cos
  * into y2_dev when non-null) element-wise, for checking against a host libm. */

@@ -203,6 +203,10 @@ _bt_set_keys = _bind("mckl_b200_batched_set_keys", [_vp, _vp, _vp, _vp])
 _LOG_PRIOR = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p)
 _pmcmc = _bind("mckl_b200_pmcmc_ar1", [_sz, _vp, _sz, _vp, _vp, _vp, _LOG_PRIOR, _vp, _sz, ctypes.c_uint32, _i,
                                        _d, _vp, _vp, _vp, _vp])
+_PROPOSAL = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.c_size_t, ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint32),
+                             ctypes.POINTER(ctypes.c_double), ctypes.c_void_p)
+_pmcmc_prop = _bind("mckl_b200_pmcmc_ar1_proposal", [_sz, _vp, _sz, _vp, _vp, _PROPOSAL, _vp, _LOG_PRIOR, _vp, _sz,
+                                                     ctypes.c_uint32, _i, _d, _vp, _vp, _vp, _vp])
 
 
 def _arr(a, dt):
@@ -429,12 +433,17 @@ class ResampleIndex:
         return int(col[id_].item())
 
 
-def pmcmc_ar1(y, N, theta0, step, log_prior, iters, seed=1, fp64=False, threshold=0.5):
+def pmcmc_ar1(y, N, theta0, step, log_prior, iters, seed=1, fp64=False, threshold=0.5, proposal=None):
     """Particle marginal Metropolis-Hastings, C chains at once
     (mckl_b200_pmcmc_ar1).  y: [C, T + 1] (or [T + 1], shared); N: particles
     per chain (int or [C]); theta0: [C, 3] = (phi, sx, sy); step: random-walk
-    scales [3]; log_prior(theta) -> float.  Returns (theta [iters, C, 3],
-    loglik [iters, C], accepted [C])."""
+    scales [3]; log_prior(theta) -> float.  `proposal(chain, iteration,
+    words, theta)`, when given, replaces the random walk
+    (mckl_b200_pmcmc_ar1_proposal, PMCMCMutation's update evaluations): it
+    changes theta (a float64 array of 3) in place from the four uint32 words
+    and returns the log proposal ratio log q(theta | theta') -
+    log q(theta' | theta).  Returns (theta [iters, C, 3], loglik [iters, C],
+    accepted [C])."""
     theta0 = _arr(np.atleast_2d(theta0), np.float64)
     C = theta0.shape[0]
     y = np.asarray(y, dtype=np.float64)
@@ -453,8 +462,19 @@ def pmcmc_ar1(y, N, theta0, step, log_prior, iters, seed=1, fp64=False, threshol
 
     cb = _LOG_PRIOR(_prior)
     vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
-    _check(_pmcmc(C, vp(Nv), T, vp(y), vp(theta0), vp(st), cb, None, iters, seed & 0xFFFFFFFF, int(bool(fp64)),
-                  threshold, vp(th), vp(ll), vp(acc), _stream_ptr()))
+    if proposal is None:
+        _check(_pmcmc(C, vp(Nv), T, vp(y), vp(theta0), vp(st), cb, None, iters, seed & 0xFFFFFFFF,
+                      int(bool(fp64)), threshold, vp(th), vp(ll), vp(acc), _stream_ptr()))
+        return th, ll, acc
+
+    def _prop(chain, it, words, theta, _user):
+        w = np.array([words[k] for k in range(4)], dtype=np.uint32)
+        t = np.ctypeslib.as_array(theta, shape=(3,))
+        return float(proposal(int(chain), int(it), w, t))
+
+    pcb = _PROPOSAL(_prop)
+    _check(_pmcmc_prop(C, vp(Nv), T, vp(y), vp(theta0), pcb, None, cb, None, iters, seed & 0xFFFFFFFF,
+                       int(bool(fp64)), threshold, vp(th), vp(ll), vp(acc), _stream_ptr()))
     return th, ll, acc
 
 

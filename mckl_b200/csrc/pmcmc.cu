@@ -15,6 +15,14 @@
 // Box-Muller on words (0, 1) and (2, 3)) and 2i + 1 (the uniform, word 0);
 // the filters of iteration i use model key (c, mix(seed, 2i)) and resampling
 // key (c, mix(seed, 2i + 1)), so every iteration draws fresh particles.
+//
+// The proposal is a hook: the reference's `update` evaluations take the
+// chain's RNG and a copy of the parameters, change the copy and return their
+// log proposal ratio (algorithm/pmcmc.hpp:116-145).  Here a proposal
+// callback gets chain c's four words of counter 2i as its randomness, the
+// copy of (phi, sx, sy) to change in place, and returns
+// log q(theta | theta') - log q(theta' | theta); the built-in Gaussian random
+// walk is the callback used when none is given (ratio 0).
 #include <cmath>
 #include <limits>
 #include <vector>
@@ -60,14 +68,48 @@ constexpr double kTwoPi = 6.283185307179586476925286766559;
 
 }  // namespace
 
+namespace {
+
+struct RandomWalk {
+    const double *step;
+};
+
+// the built-in proposal: theta + step * (three standard normals by
+// Box-Muller from the four words), symmetric
+double random_walk(size_t, size_t, const uint32_t w[4], double *theta, void *user)
+{
+    const double *step = static_cast<const RandomWalk *>(user)->step;
+    const double r0 = std::sqrt(-2.0 * std::log((w[0] + 1.0) * 0x1p-32));
+    const double a0 = kTwoPi * (w[1] * 0x1p-32);
+    const double r1 = std::sqrt(-2.0 * std::log((w[2] + 1.0) * 0x1p-32));
+    const double a1 = kTwoPi * (w[3] * 0x1p-32);
+    const double z[3] = {r0 * std::cos(a0), r0 * std::sin(a0), r1 * std::cos(a1)};
+    for (int k = 0; k < 3; ++k) theta[k] = theta[k] + step[k] * z[k];
+    return 0.0;
+}
+
+}  // namespace
+
 extern "C" int mckl_b200_pmcmc_ar1(size_t C, const size_t *N, size_t T, const double *y, const double *theta0,
     const double *step, mckl_b200_log_prior_t prior, void *user, size_t iters, uint32_t seed, int fp64,
     double threshold, double *theta_out, double *loglik_out, uint32_t *accepted, void *stream)
 {
+    MB_CHECK_ARG(step != nullptr, "null step");
+    RandomWalk rw{step};
+    return mckl_b200_pmcmc_ar1_proposal(C, N, T, y, theta0, random_walk, &rw, prior, user, iters, seed, fp64,
+        threshold, theta_out, loglik_out, accepted, stream);
+}
+
+extern "C" int mckl_b200_pmcmc_ar1_proposal(size_t C, const size_t *N, size_t T, const double *y,
+    const double *theta0, mckl_b200_proposal_t proposal, void *proposal_user, mckl_b200_log_prior_t prior,
+    void *user, size_t iters, uint32_t seed, int fp64, double threshold, double *theta_out, double *loglik_out,
+    uint32_t *accepted, void *stream)
+{
     using namespace mckl_b200;
-    MB_CHECK_ARG(C > 0 && N && T > 0 && y && theta0 && step && prior && iters > 0, "bad arguments");
+    MB_CHECK_ARG(C > 0 && N && T > 0 && y && theta0 && proposal && prior && iters > 0, "bad arguments");
     MB_CHECK_ARG(theta_out && loglik_out && accepted, "null output");
     MB_CHECK_ARG(fp64 == 0 || fp64 == 1, "fp64: 0 (FP32 moves) or 1 (FP64)");
+    std::vector<double> lq(C, 0.0);
     std::vector<double> phi(C), sx(C), sy(C), lp(C), ll(C), th(3 * C), thp(3 * C);
     std::vector<uint32_t> mk(2 * C), rk(2 * C), nres(C);
     std::vector<char> valid(C);
@@ -106,15 +148,11 @@ extern "C" int mckl_b200_pmcmc_ar1(size_t C, const size_t *N, size_t T, const do
             for (size_t c = 0; c < C; ++c) {
                 uint32_t w[4];
                 philox_host(seed, static_cast<uint32_t>(c), 2 * it, w);
-                const double r0 = std::sqrt(-2.0 * std::log((w[0] + 1.0) * 0x1p-32));
-                const double a0 = kTwoPi * (w[1] * 0x1p-32);
-                const double r1 = std::sqrt(-2.0 * std::log((w[2] + 1.0) * 0x1p-32));
-                const double a1 = kTwoPi * (w[3] * 0x1p-32);
-                const double z[3] = {r0 * std::cos(a0), r0 * std::sin(a0), r1 * std::cos(a1)};
-                for (int k = 0; k < 3; ++k) thp[3 * c + k] = th[3 * c + k] + step[k] * z[k];
+                for (int k = 0; k < 3; ++k) thp[3 * c + k] = th[3 * c + k];
+                lq[c] = proposal(c, it, w, &thp[3 * c], proposal_user);
                 const bool in_model = thp[3 * c] * thp[3 * c] < 1 && thp[3 * c + 1] > 0 && thp[3 * c + 2] > 0;
                 lp[c] = in_model ? prior(&thp[3 * c], user) : -std::numeric_limits<double>::infinity();
-                valid[c] = std::isfinite(lp[c]) ? 1 : 0;
+                valid[c] = std::isfinite(lp[c]) && std::isfinite(lq[c]) ? 1 : 0;
                 // a proposal outside the support is rejected without a filter
                 // run: its filter reruns the current parameters
                 const double *src = valid[c] ? &thp[3 * c] : &th[3 * c];
@@ -134,7 +172,7 @@ extern "C" int mckl_b200_pmcmc_ar1(size_t C, const size_t *N, size_t T, const do
                 const double logu = std::log((w[0] + 0.5) * 0x1p-32);
                 const double lp_old = prior(&th[3 * c], user);
                 double prob = -lp_old - ll_cur[c];
-                prob += 0.0;  // symmetric random walk: the proposal ratio is 1
+                prob += lq[c];  // the proposal's log ratio (the reference's sum of evaluations)
                 prob += lp[c];
                 prob += ll[c];
                 if (logu < prob) {
