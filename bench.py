@@ -513,6 +513,48 @@ def bench_adjoint(rank, dev, sets=256, N=1 << 16, T=1000, C=32, threads=1024):
     rel_k = np.linalg.norm(g - kg, axis=1) / np.linalg.norm(kg, axis=1)
     cos = np.sum(g * kg, axis=1) / (np.linalg.norm(g, axis=1) * np.linalg.norm(kg, axis=1))
     ps = float(sets) * N * T
+    # both estimators over R independent runs (model and resampling keys):
+    # the fixed-ancestor adjoint and the consistent score (Fisher identity,
+    # PaRIS), each against the Kalman gradient with its Monte Carlo error
+    R, score_threads = 8, 512
+    b = mb.BatchedFilters(w["N"], w["y"], w["phi"], w["sx"], w["sy"], w["mkeys"], w["rkeys"], fp64=True)
+    S = np.zeros((R, sets, 3))
+    G = np.zeros((R, sets, 3))
+    score_ms = []
+    for r in range(R):
+        mk, rk = w["mkeys"].copy(), w["rkeys"].copy()
+        mk[:, 1] += 1000 * (r + 1)
+        rk[:, 1] += 1000 * (r + 1)
+        b.set_keys(mk, rk)
+        b.config(score_threads, 1)
+        e0, e1 = events()
+        e0.record(stream)
+        _, S[r] = b.score()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        score_ms.append(e0.elapsed_time(e1))
+        b.config(threads, 1)
+        _, G[r] = b.adjoint(C)
+    b.close()
+
+    def vs_kalman(E):
+        mean = E.mean(0)
+        se = E.std(0, ddof=1) / np.sqrt(R)
+        kn = np.linalg.norm(kg, axis=1)
+        single = np.linalg.norm(E - kg[None], axis=2) / kn[None]
+        return {"rel_norm_of_mean_median": float(np.median(np.linalg.norm(mean - kg, axis=1) / kn)),
+                "rel_norm_single_run_median": float(np.median(single)),
+                "rel_se_of_mean_median": float(np.median(np.linalg.norm(se, axis=1) / kn)),
+                "components_within_3se": float(np.mean(np.abs(mean - kg) <= 3 * se))}
+
+    estimators = {
+        "runs": R,
+        "adjoint_fixed_ancestors": vs_kalman(G),
+        "score_fisher_paris": dict(vs_kalman(S), ms_per_run=float(np.median(score_ms)),
+                                   threads=score_threads),
+        "definition": "per parameter set: ||mean over runs - Kalman|| / ||Kalman|| (median over sets), the same "
+                      "for single runs, the standard error of the mean relative to ||Kalman||, and the fraction "
+                      "of components whose mean lies within 3 standard errors of Kalman"}
     return {"workload": f"{sets} parameter sets, N = {N}, T = {T}, FP64, checkpoint every {C} steps, "
                         f"{threads} threads per filter",
             "ms": ms, "forward_particle_steps_per_s": ps / (ms / 1e3),
@@ -524,7 +566,8 @@ def bench_adjoint(rank, dev, sets=256, N=1 << 16, T=1000, C=32, threads=1024):
                                      "definition": "same, against (4 FD(h/2) - FD(h)) / 3"},
             "vs_kalman": {"rel_norm_median": float(np.median(rel_k)), "cosine_median": float(np.median(cos)),
                           "loglik_minus_kalman_mean": float(np.mean(ll - kll)),
-                          "note": "fixed ancestors: a biased estimate of the exact score at any N"}}
+                          "note": "fixed ancestors: a biased estimate of the exact score at any N"},
+            "estimators_vs_kalman": estimators}
 
 
 # ---------------------------------------------------------------------------

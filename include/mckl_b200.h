@@ -280,6 +280,19 @@ int mckl_b200_batched_shadow_params(mckl_b200_batched_t *b, const double *phi, c
 int mckl_b200_batched_adjoint(mckl_b200_batched_t *b, int checkpoint_every, double *loglik, double *grad,
                               void *stream);
 
+/* Score estimate by the Fisher identity (no counterpart in the reference):
+ * grad log p(y_1:T | theta) = E[grad log p(x_0:T, y_1:T | theta) | y_1:T],
+ * estimated in the same forward pass as each filter's FP64 log-likelihood by
+ * PaRIS (per-particle statistics updated from two backward draws per step, an
+ * independent Metropolis-Hastings chain started at the particle's ancestor).
+ * Unlike the adjoint, which differentiates the estimate with the ancestors
+ * held fixed, this is a consistent estimate of the exact score: its error
+ * against the Kalman gradient is Monte Carlo error that falls as N grows.
+ * Handle created with fp64 = 1.  loglik: F doubles (may be NULL), score:
+ * F x 3 doubles (d/dphi, d/dsx, d/dsy), HOST arrays; synchronizes `stream`.
+ * Device memory: 80 B x the largest N per SM. */
+int mckl_b200_batched_score(mckl_b200_batched_t *b, double *loglik, double *score, void *stream);
+
 /* Autotuner: times the candidate block shapes (threads per CTA x resident CTAs
  * per SM, skipping shapes that do not fit) on this handle's own filters, one
  * full run each, and configures the fastest.  The first `max_trials` trials

@@ -198,6 +198,7 @@ _bt_set_y = _bind("mckl_b200_batched_set_y", [_vp, _vp, _vp])
 _bt_autotune = _bind("mckl_b200_batched_autotune", [_vp, _i, _vp, _vp, _vp, _vp, _vp])
 _bt_shadow_params = _bind("mckl_b200_batched_shadow_params", [_vp, _vp, _vp, _vp])
 _bt_adjoint = _bind("mckl_b200_batched_adjoint", [_vp, _i, _vp, _vp, _vp])
+_bt_score = _bind("mckl_b200_batched_score", [_vp, _vp, _vp, _vp])
 _bt_set_params = _bind("mckl_b200_batched_set_params", [_vp, _vp, _vp, _vp, _vp])
 _bt_set_keys = _bind("mckl_b200_batched_set_keys", [_vp, _vp, _vp, _vp])
 _LOG_PRIOR = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p)
@@ -266,6 +267,16 @@ class BatchedFilters:
         g = np.zeros((self.F, 3))
         _check(_bt_adjoint(self.h, int(checkpoint_every), ll.ctypes.data_as(ctypes.c_void_p),
                            g.ctypes.data_as(ctypes.c_void_p), _stream_ptr(stream)))
+        return ll, g
+
+    def score(self, stream=None):
+        """(loglik[F], score[F, 3]): the FP64 estimate and a consistent
+        estimate of the score d log p(y | theta) / d (phi, sx, sy) by the
+        Fisher identity (PaRIS smoothing in the same pass; fp64=True handles)."""
+        ll = np.zeros(self.F)
+        g = np.zeros((self.F, 3))
+        _check(_bt_score(self.h, ll.ctypes.data_as(ctypes.c_void_p), g.ctypes.data_as(ctypes.c_void_p),
+                         _stream_ptr(stream)))
         return ll, g
 
     def set_params(self, phi, sx, sy, stream=None):

@@ -1033,6 +1033,188 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_adjoint(const BatchedFilter *
     }
 }
 
+// ---------------------------------------------------------------------------
+// Score by the Fisher identity: grad log p(y_1:T) = E[grad log p(x_0:T, y_1:T)
+// | y_1:T], the expectation of an additive functional of the path, estimated
+// forward with PaRIS (Olsson and Westerborn 2017, "Efficient particle-based
+// online smoothing in general hidden Markov models: the PaRIS algorithm").
+// Each particle i of the cloud at t carries tau_t^i, an estimate of
+// E[sum_{s<=t} s_s | x_t = xi_t^i, y_1:t]:
+//   tau_0^i = s_0(xi_0^i),
+//   tau_t^i = (1/K) sum_k [tau_{t-1}^{J_k} + s_t(x_{t-1}^{J_k}, xi_t^i)],
+// the J_k drawn from the backward kernel, probability proportional to
+// W_{t-1}^j f(xi_t^i | x_{t-1}^j) over the weighted cloud at t - 1 (before its
+// resampling).  The J_k are K = 2 steps of an independent Metropolis-Hastings
+// chain started at the particle's own ancestor (Dau and Chopin 2022, "On
+// backward smoothing algorithms"), the proposal being the ancestor of a
+// uniformly drawn slot: q(j) = rep_j / N, rep_j the copies of j after the
+// resampling (1 without one), so the acceptance ratio is
+//   W_j' f(xi | x_j') rep_J / (W_J f(xi | x_J) rep_j').
+// The estimate is sum_i W_T^i tau_T^i.  Additive terms, theta = (phi, sx, sy):
+//   transition  d = x_t - phi x_{t-1}:  (d x_{t-1} / sx^2, -1/sx + d^2 / sx^3, 0)
+//   observation r = y_t - x_t:           (0, 0, -1/sy + r^2 / sy^3)
+//   initial     x_0 ~ N(0, sd0^2), sd0 = sx / sqrt(1 - phi^2):
+//               v = x_0^2 / sd0^2 - 1:   (v phi / (1 - phi^2), v / sx, 0)
+// The backward draws use Philox4x32 with the filter's resampling key, its
+// second word xor 0x9E3779B9, counter (i, t): one block per particle and
+// step (slot index and acceptance uniform of each of the two moves).
+// ---------------------------------------------------------------------------
+struct ScoreArgs {
+    uint64_t nmax;
+    double *xb;            // 2 x nmax per CTA: clouds at t - 1 and t before their resampling
+    double *w;             // nmax per CTA: normalised weights of the cloud at t - 1
+    uint32_t *rep, *anc;   // nmax per CTA: copies of each particle at t - 1, parent of each slot
+    double *tau;           // 2 x 3 x nmax per CTA (component-major)
+    double *score;         // 3 per filter
+};
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 1) k_pf_score(const BatchedFilter *filt, const int *order, int nf,
+    const double *y, int T, double threshold, double *xa, double *xb, double *lw, uint32_t *scanS, uint32_t *epos,
+    double *loglik, uint32_t *nresampled, int *queue, ScoreArgs A)
+{
+    __shared__ double shd[33];
+    __shared__ unsigned long long shu[33];
+    __shared__ __align__(16) uint32_t shj[shj_words<THREADS>()];
+    __shared__ int sh_f;
+    const uint64_t slot = blockIdx.x, nm = A.nmax;
+    double *xbuf[2] = {A.xb + slot * 2 * nm, A.xb + slot * 2 * nm + nm};
+    double *W = A.w + slot * nm;
+    uint32_t *rep = A.rep + slot * nm, *anc = A.anc + slot * nm;
+    double *taub[2] = {A.tau + slot * 6 * nm, A.tau + slot * 6 * nm + 3 * nm};
+    while (true) {
+        if (threadIdx.x == 0) {
+            const int k = atomicAdd(queue, 1);
+            sh_f = k < nf ? order[k] : -1;
+        }
+        __syncthreads();
+        const int f = sh_f;
+        __syncthreads();
+        if (f < 0) break;
+        const BatchedFilter F = filt[f];
+        const uint64_t N = F.n;
+        const uint32_t N32 = static_cast<uint32_t>(N);
+        const double *yf = y + static_cast<uint64_t>(f) * (T + 1);
+        const double phi = F.phi, sx = F.sx, sy = F.sy;
+        const double isx2 = 1.0 / (sx * sx), hsx2 = 0.5 * isx2;
+        const double q0 = 1.0 - phi * phi, isd02 = q0 * isx2;
+        const PhiloxGen gb{F.rkey[0], F.rkey[1] ^ 0x9E3779B9u};
+        FilterRun<double, THREADS, false> run;
+        run.setup(F, xa, xb, lw, scanS, epos, nullptr, nullptr, nullptr, threshold);
+        // t = 0: the initial cloud, equal weights, no resampling
+        run.step(0, yf[0], shd, shd, shu, shj);
+        for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
+            const double x0 = run.xc[p];
+            const double v = x0 * x0 * isd02 - 1.0;
+            xbuf[0][p] = x0;
+            W[p] = 1.0 / static_cast<double>(N);
+            rep[p] = 1;
+            anc[p] = static_cast<uint32_t>(p);
+            taub[0][p] = v * phi / q0;
+            taub[0][nm + p] = v / sx;
+            taub[0][2 * nm + p] = 0.0;
+        }
+        __syncthreads();
+        int cur = 0;
+        for (int t = 1; t <= T; ++t) {
+            double *xprev = xbuf[(t - 1) & 1], *xnow = xbuf[t & 1];
+            run.rec_x = xnow;  // the step records its cloud before resampling
+            const bool res = run.step(t, yf[t], shd, shd, shu, shj);
+            run.rec_x = nullptr;
+            // PaRIS update of every particle of the cloud at t
+            const double *tp = taub[cur];
+            double *tn = taub[cur ^ 1];
+            const double yt = yf[t];
+            for (uint64_t i = threadIdx.x; i < N; i += THREADS) {
+                const double xi = xnow[i];
+                uint32_t wd[4];
+                gb.block(Ctr{{i, static_cast<uint64_t>(t), 0, 0}}, wd);
+                uint32_t J = anc[i];
+                double dJ = xi - phi * xprev[J];
+                double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+#pragma unroll
+                for (int m = 0; m < 2; ++m) {
+                    const uint32_t k = static_cast<uint32_t>((static_cast<uint64_t>(wd[2 * m]) * N32) >> 32);
+                    const uint32_t jp = anc[k];
+                    const double dp = xi - phi * xprev[jp];
+                    // log of the acceptance ratio
+                    const double lr = (dJ * dJ - dp * dp) * hsx2 + log(W[jp] * rep[J]) - log(W[J] * rep[jp]);
+                    const double u = (static_cast<double>(wd[2 * m + 1]) + 0.5) * 0x1p-32;
+                    if (log(u) < lr) {
+                        J = jp;
+                        dJ = dp;
+                    }
+                    const double xJ = xprev[J];
+                    a0 += tp[J] + dJ * xJ * isx2;
+                    a1 += tp[nm + J] + (dJ * dJ * isx2 - 1.0) / sx;
+                    a2 += tp[2 * nm + J];
+                }
+                const double r = yt - xi;
+                tn[i] = 0.5 * a0;
+                tn[nm + i] = 0.5 * a1;
+                tn[2 * nm + i] = 0.5 * a2 + (r * r / (sy * sy) - 1.0) / sy;
+            }
+            cur ^= 1;
+            __syncthreads();
+            // the cloud at t for the next step: normalised weights (the
+            // log-weights are left as they were before the resampling) and,
+            // when it was resampled, the parents of the slots
+            double mx = -INFINITY;
+            for (uint64_t p = threadIdx.x; p < N; p += THREADS) mx = fmax(mx, run.st.l[p]);
+            mx = block_max(mx, shd);
+            double ssum = 0.0;
+            for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
+                const double e = exp(run.st.l[p] - mx);
+                W[p] = e;
+                ssum += e;
+                anc[p] = static_cast<uint32_t>(p);
+            }
+            ssum = block_sum(ssum, shd);
+            const double inv = 1.0 / ssum;
+            for (uint64_t p = threadIdx.x; p < N; p += THREADS) W[p] *= inv;
+            __syncthreads();
+            if (res) {
+                // slot-preserving placement: parent p keeps slot p when it
+                // has copies and fills the empties ep[sS_p .. sS_{p+1})
+                const uint32_t ne = static_cast<uint32_t>(run.n_empty);
+                for (uint32_t k = threadIdx.x; k < ne; k += THREADS) anc[run.ep[k]] = 0xFFFFFFFFu;
+                __syncthreads();
+                for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
+                    const uint32_t b = run.sS[p], e = p + 1 < N ? run.sS[p + 1] : ne;
+                    for (uint32_t c = b; c < e; ++c) anc[run.ep[c]] = static_cast<uint32_t>(p);
+                }
+                __syncthreads();
+                for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
+                    const uint32_t b = run.sS[p], e = p + 1 < N ? run.sS[p + 1] : ne;
+                    rep[p] = (anc[p] == p ? 1u : 0u) + (e - b);
+                }
+            } else {
+                for (uint64_t p = threadIdx.x; p < N; p += THREADS) rep[p] = 1;
+            }
+            __syncthreads();
+        }
+        // the estimate: sum_i W_T^i tau_T^i
+        double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+        const double *tT = taub[cur];
+        for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
+            g0 += W[p] * tT[p];
+            g1 += W[p] * tT[nm + p];
+            g2 += W[p] * tT[2 * nm + p];
+        }
+        g0 = block_sum(g0, shd);
+        g1 = block_sum(g1, shd);
+        g2 = block_sum(g2, shd);
+        if (threadIdx.x == 0) {
+            loglik[f] = run.ll_sum;
+            nresampled[f] = static_cast<uint32_t>(run.events);
+            A.score[3 * f] = g0;
+            A.score[3 * f + 1] = g1;
+            A.score[3 * f + 2] = g2;
+        }
+        __syncthreads();
+    }
+}
+
 // Two register budgets per block shape: MINB = 1 (the compiler's choice, 16
 // warps per SM at most) and MINB = 1024 / THREADS (64 registers, 32 warps).
 template <typename R, int THREADS, bool SHADOW, int MINB>
@@ -1125,6 +1307,29 @@ int pf_adjoint_launch(const BatchedArgs &a, const int *order, int nf, int thread
     }
 }
 
+template <int THREADS>
+int score_one(const BatchedArgs &a, const int *order, int nf, int *queue, const ScoreArgs &A, int ctas,
+    cudaStream_t s)
+{
+    k_pf_score<THREADS><<<ctas, THREADS, 0, s>>>(a.filt, order, nf, a.y, a.T, a.threshold,
+        static_cast<double *>(a.xa), static_cast<double *>(a.xb), static_cast<double *>(a.lw), a.scanS, a.epos,
+        a.loglik, a.nresampled, queue, A);
+    MB_LAUNCH_CHECK();
+    return MCKL_B200_OK;
+}
+
+int pf_score_launch(const BatchedArgs &a, const int *order, int nf, int threads, int *queue, const ScoreArgs &A,
+    int ctas, cudaStream_t s)
+{
+    MB_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), s));
+    switch (threads) {
+        case 128: return score_one<128>(a, order, nf, queue, A, ctas, s);
+        case 256: return score_one<256>(a, order, nf, queue, A, ctas, s);
+        case 512: return score_one<512>(a, order, nf, queue, A, ctas, s);
+        default: return score_one<1024>(a, order, nf, queue, A, ctas, s);
+    }
+}
+
 int pf_batched_launch(const BatchedArgs &a, const int *order, int nf, int threads, int ctas_per_sm, int *queue,
     cudaStream_t s)
 {
@@ -1161,6 +1366,8 @@ struct mckl_b200_batched {
     uint64_t nmax = 0;                         // largest particle count
     void *adj_mem = nullptr;                   // adjoint checkpoints and work areas
     size_t adj_bytes = 0;
+    void *score_mem = nullptr;                 // score estimator work areas
+    size_t score_bytes = 0;
 };
 
 using namespace mckl_b200;
@@ -1499,9 +1706,54 @@ int mckl_b200_batched_adjoint(mckl_b200_batched_t *b, int checkpoint_every, doub
     return MCKL_B200_OK;
 }
 
+int mckl_b200_batched_score(mckl_b200_batched_t *b, double *loglik, double *score, void *stream)
+{
+    MB_CHECK_ARG(b != nullptr && score != nullptr, "null argument");
+    MB_CHECK_ARG(b->fp64 == 1 && b->a.xsa == nullptr, "the score needs a handle created with fp64 = 1");
+    cudaStream_t s = as_stream(stream);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int ctas = std::max(1, std::min(b->F, sms));
+    const uint64_t nm = b->nmax;
+    const size_t need = align256(ctas * 2 * nm * 8) + align256(ctas * nm * 8) + 2 * align256(ctas * nm * 4) +
+                        align256(ctas * 6 * nm * 8) + align256(static_cast<size_t>(b->F) * 24);
+    if (b->score_bytes < need) {
+        if (b->score_mem) cudaFree(b->score_mem);
+        b->score_mem = nullptr;
+        b->score_bytes = 0;
+        if (cudaMalloc(&b->score_mem, need) != cudaSuccess) {
+            set_error("score work memory (" + std::to_string(need >> 20) + " MiB) could not be allocated");
+            return MCKL_B200_ERR_NOMEM;
+        }
+        b->score_bytes = need;
+    }
+    char *p = static_cast<char *>(b->score_mem);
+    auto take = [&p](size_t n) {
+        char *q = p;
+        p += align256(n);
+        return q;
+    };
+    ScoreArgs A{};
+    A.nmax = nm;
+    A.xb = reinterpret_cast<double *>(take(ctas * 2 * nm * 8));
+    A.w = reinterpret_cast<double *>(take(ctas * nm * 8));
+    A.rep = reinterpret_cast<uint32_t *>(take(ctas * nm * 4));
+    A.anc = reinterpret_cast<uint32_t *>(take(ctas * nm * 4));
+    A.tau = reinterpret_cast<double *>(take(ctas * 6 * nm * 8));
+    A.score = reinterpret_cast<double *>(take(static_cast<size_t>(b->F) * 24));
+    int rc = pf_score_launch(b->a, b->order, b->F, b->threads, b->queue, A, ctas, s);
+    if (rc != MCKL_B200_OK) return rc;
+    if (loglik) MB_CUDA(cudaMemcpyAsync(loglik, b->a.loglik, b->F * 8, cudaMemcpyDeviceToHost, s));
+    MB_CUDA(cudaMemcpyAsync(score, A.score, static_cast<size_t>(b->F) * 24, cudaMemcpyDeviceToHost, s));
+    MB_CUDA(cudaStreamSynchronize(s));
+    return MCKL_B200_OK;
+}
+
 int mckl_b200_batched_destroy(mckl_b200_batched_t *b)
 {
     if (!b) return MCKL_B200_OK;
+    if (b->score_mem) cudaFree(b->score_mem);
     if (b->adj_mem) cudaFree(b->adj_mem);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
