@@ -321,7 +321,7 @@ __device__ __forceinline__ void st8(uint32_t *p, const uint32_t (&v)[8])
 }
 
 struct NoiseLayout {
-    static constexpr uint64_t kUnits = 129;  // units per full chunk
+    static constexpr uint64_t kUnits = 129;  // units per full chunk (the 32-bit division below uses 129)
     uint64_t N, m, tail, nu_tail, units, per_step;
 
     __device__ void init(uint64_t n)
@@ -343,7 +343,9 @@ struct NoiseLayout {
     {
         const uint64_t P = static_cast<uint64_t>(t) * per_step;
         if (u < m * kUnits) {
-            const uint64_t c = u / kUnits, g = u % kUnits;
+            // u < 2^28 (N < 2^31): 32-bit division by the constant
+            const uint32_t u32 = static_cast<uint32_t>(u), c32 = u32 / 129u;
+            const uint64_t c = c32, g = u32 - c32 * 129u;
             const uint64_t base = P + c * 1024;
             const uint64_t B = (base >> 2) + g;
             const int i0 = static_cast<int>(4 * g) - static_cast<int>(base & 3);
@@ -378,7 +380,9 @@ struct NoiseLayout {
     {
         const uint64_t P = static_cast<uint64_t>(t) * per_step;
         if (u < m * kUnits) {
-            const uint64_t c = u / kUnits, g = u % kUnits;
+            // u < 2^28 (N < 2^31): 32-bit division by the constant
+            const uint32_t u32 = static_cast<uint32_t>(u), c32 = u32 / 129u;
+            const uint64_t c = c32, g = u32 - c32 * 129u;
             const uint64_t base = P + c * 1024;
             const uint64_t B = (base >> 2) + g;
             const int i0 = static_cast<int>(4 * g) - static_cast<int>(base & 3);
@@ -512,7 +516,7 @@ struct FilterRun {
         Lse<R> acc;
         Lse<double> accs;
         // ---- noise, propagation, log-weights, online normaliser
-        for (uint64_t u = threadIdx.x; u < lay.units; u += THREADS) {
+        for (uint32_t u = threadIdx.x; u < static_cast<uint32_t>(lay.units); u += THREADS) {
             R v[8];
             double vs[8];
             int lo, hi;
@@ -895,7 +899,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_adjoint(const BatchedFilter *
         // noise of step t paired with lambda: sum_j lambda_j eps_j
         auto lam_eps = [&](int t) {
             double acc = 0.0;
-            for (uint64_t u = threadIdx.x; u < run.lay.units; u += THREADS) {
+            for (uint32_t u = threadIdx.x; u < static_cast<uint32_t>(run.lay.units); u += THREADS) {
                 int lo, hi;
                 run.lay.unit(run.gm, t, u, &lo, &hi, [&](uint32_t wrad, uint32_t wang, uint64_t p0, uint64_t p1, int) {
                     const double r = Math<double>::radius(u01oc<double>(wrad));
