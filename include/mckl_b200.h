@@ -297,10 +297,15 @@ int mckl_b200_batched_score(mckl_b200_batched_t *b, double *loglik, double *scor
  * per SM, skipping shapes that do not fit) on this handle's own filters, one
  * full run each, and configures the fastest.  The first `max_trials` trials
  * are reported in threads[] / ctas_per_sm[] / ms[] (any may be NULL); the
- * number of trials in *ntrials.  Synchronizes `stream`. */
+ * number of trials in *ntrials.  The pick is kept for the process: a later
+ * handle with the same workload (device, precision mode, filter count, steps,
+ * threshold and particle counts) is configured from it without timing
+ * (*ntrials = 0).  Synchronizes `stream` when it times. */
 int mckl_b200_batched_autotune(mckl_b200_batched_t *b, int max_trials, int *threads, int *ctas_per_sm, float *ms,
                                int *ntrials, void *stream);
 int mckl_b200_batched_set_y(mckl_b200_batched_t *b, const double *y, void *stream);
+/* The block shape the handle runs with (set by _config or the autotuner). */
+int mckl_b200_batched_get_config(const mckl_b200_batched_t *b, int *threads, int *ctas_per_sm);
 int mckl_b200_batched_destroy(mckl_b200_batched_t *b);
 
 /* Sequential left fold s_i = s_{i-1} + x_i (s_{-1} = s0) of n nonnegative

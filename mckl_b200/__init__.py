@@ -196,6 +196,7 @@ _bt_destroy = _bind("mckl_b200_batched_destroy", [_vp])
 _bt_shadow = _bind("mckl_b200_batched_shadow", [_vp, _vp, _vp])
 _bt_set_y = _bind("mckl_b200_batched_set_y", [_vp, _vp, _vp])
 _bt_autotune = _bind("mckl_b200_batched_autotune", [_vp, _i, _vp, _vp, _vp, _vp, _vp])
+_bt_get_config = _bind("mckl_b200_batched_get_config", [_vp, _vp, _vp])
 _bt_shadow_params = _bind("mckl_b200_batched_shadow_params", [_vp, _vp, _vp, _vp])
 _bt_adjoint = _bind("mckl_b200_batched_adjoint", [_vp, _i, _vp, _vp, _vp])
 _bt_score = _bind("mckl_b200_batched_score", [_vp, _vp, _vp, _vp])
@@ -247,13 +248,23 @@ class BatchedFilters:
 
     def autotune(self, stream=None):
         """Time the candidate block shapes on these filters and keep the
-        fastest; returns [(threads, ctas_per_sm, ms), ...]."""
+        fastest; returns [(threads, ctas_per_sm, ms), ...].  A workload tuned
+        before in this process is configured from the kept pick without
+        timing: then the one entry is that pick with ms = nan."""
         th = (ctypes.c_int * 16)()
         cp = (ctypes.c_int * 16)()
         ms = (ctypes.c_float * 16)()
         n = ctypes.c_int()
         _check(_bt_autotune(self.h, 16, th, cp, ms, ctypes.byref(n), _stream_ptr(stream)))
+        if n.value == 0:
+            return [self.shape() + (float("nan"),)]
         return [(th[k], cp[k], ms[k]) for k in range(min(n.value, 16))]
+
+    def shape(self):
+        """(threads per CTA, resident CTAs per SM) the handle runs with."""
+        t, c = ctypes.c_int(), ctypes.c_int()
+        _check(_bt_get_config(self.h, ctypes.byref(t), ctypes.byref(c)))
+        return (t.value, c.value)
 
     def set_shadow_params(self, phi, sx, sy):
         """Parameters of the FP64 shadow (handles made with shadow=True)."""

@@ -20,6 +20,9 @@
 // Particle state (x, log-weights) lives in global memory, contiguous per
 // filter; only the filters in flight are touched, so it stays in L2.
 #include <algorithm>
+#include <cstring>
+#include <map>
+#include <mutex>
 #include <cmath>
 #include <vector>
 
@@ -1378,6 +1381,33 @@ using namespace mckl_b200;
 
 namespace {
 
+// Autotuner picks of this process, by workload: FNV-1a over the device, the
+// precision mode, F, T, the threshold and every particle count.
+std::mutex g_tune_mu;
+std::map<uint64_t, std::pair<int, int>> g_tune;
+
+uint64_t tune_key(const mckl_b200_batched *b)
+{
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&h](uint64_t v) {
+        for (int k = 0; k < 8; ++k) {
+            h ^= (v >> (8 * k)) & 0xFF;
+            h *= 1099511628211ull;
+        }
+    };
+    int dev = 0;
+    cudaGetDevice(&dev);
+    uint64_t thr;
+    std::memcpy(&thr, &b->threshold, sizeof(thr));
+    mix(static_cast<uint64_t>(dev));
+    mix(static_cast<uint64_t>(b->fp64) | (b->a.xsa ? 2u : 0u));
+    mix(static_cast<uint64_t>(b->F));
+    mix(static_cast<uint64_t>(b->T));
+    mix(thr);
+    for (const auto &f : b->hf) mix(f.n);
+    return h;
+}
+
 // main-run parameters of one filter and their derived constants
 void set_main(BatchedFilter &h, double phi, double sx, double sy)
 {
@@ -1498,6 +1528,14 @@ int mckl_b200_batched_config(mckl_b200_batched_t *b, int threads, int ctas_per_s
     return MCKL_B200_OK;
 }
 
+int mckl_b200_batched_get_config(const mckl_b200_batched_t *b, int *threads, int *ctas_per_sm)
+{
+    MB_CHECK_ARG(b != nullptr, "null handle");
+    if (threads) *threads = b->threads;
+    if (ctas_per_sm) *ctas_per_sm = b->ctas_per_sm;
+    return MCKL_B200_OK;
+}
+
 int mckl_b200_batched_run(mckl_b200_batched_t *b, void *stream)
 {
     MB_CHECK_ARG(b != nullptr, "null handle");
@@ -1531,6 +1569,17 @@ int mckl_b200_batched_autotune(mckl_b200_batched_t *b, int max_trials, int *thre
 {
     MB_CHECK_ARG(b != nullptr && max_trials >= 0, "bad arguments");
     cudaStream_t s = as_stream(stream);
+    // a workload tuned before in this process (same device, precision mode,
+    // filter count, steps, threshold and particle counts) reuses its pick
+    const uint64_t key = tune_key(b);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) {
+            if (ntrials) *ntrials = 0;
+            return mckl_b200_batched_config(b, it->second.first, it->second.second);
+        }
+    }
     // candidate block shapes: 16 or 32 resident warps per SM (the latter with
     // the register-capped variant), from many small CTAs (small filters keep
     // every thread busy) to few large ones (fewer barriers per particle)
@@ -1575,6 +1624,10 @@ int mckl_b200_batched_autotune(mckl_b200_batched_t *b, int max_trials, int *thre
     if (ntrials) *ntrials = n;
     if (rc != MCKL_B200_OK) return rc;
     MB_CHECK_ARG(best >= 0, "autotune: no candidate block shape fits");
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune[key] = {cand[best][0], cand[best][1]};
+    }
     return mckl_b200_batched_config(b, cand[best][0], cand[best][1]);
 }
 

@@ -95,6 +95,12 @@ def test_batched_autotune_and_set_y(env, small):
     trials = b.autotune()
     assert len(trials) >= 2 and all(ms > 0 for (_, _, ms) in trials)
     best = min(trials, key=lambda r: r[2])
+    assert b.shape() == (best[0], best[1])
+    # the pick is kept for the workload: a second handle is configured from it without timing
+    b2 = mb.BatchedFilters(w["N"], w["y"], w["phi"], w["sx"], w["sy"], w["mkeys"], w["rkeys"])
+    again = b2.autotune()
+    assert len(again) == 1 and again[0][:2] == best[:2] and b2.shape() == best[:2]
+    b2.close()
     b.run(graph=True)
     ll, nr = b.results()
     ref = mb.BatchedFilters(w["N"], w["y"], w["phi"], w["sx"], w["sy"], w["mkeys"], w["rkeys"])
