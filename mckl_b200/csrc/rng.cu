@@ -246,8 +246,8 @@ __device__ __forceinline__ bool store_warp32(R *out, uint64_t b, uint64_t nblk, 
 
 // Aligned shape: nblk whole blocks starting at counter `base`; block b feeds
 // outputs [b * OPB, (b + 1) * OPB).  `out` is 16-byte aligned.
-template <class G, typename W, class F>
-__global__ void __launch_bounds__(256) k_blocks(G g, Ctr base, uint64_t nblk, typename F::out_t *out, F f)
+template <class G, typename W, class F, int THREADS = 256>
+__global__ void __launch_bounds__(THREADS) k_blocks(G g, Ctr base, uint64_t nblk, typename F::out_t *out, F f)
 {
     using R = typename F::out_t;
     constexpr int WPB = G::kWords / WordView<W>::kPer32;  // words per block
@@ -462,6 +462,16 @@ static int launch_words(const G &g, const Ctr &B, uint32_t off, uint64_t n, type
             // no carry out of the low counter word within this launch
             if (nblk && (B.w[0] & 0xffffffffull) + (nblk - 1) <= 0xffffffffull) {
                 k_blocks_plo<W, F><<<grid_for(nblk, 256, ctas), 256, 0, s>>>(PhiloxLo::make(g, B), nblk, out, f);
+                MB_LAUNCH_CHECK();
+                done_blocks = true;
+            }
+        }
+        if constexpr (std::is_same<G, ArsGen>::value) {
+            // ARS with four round tables: one 1024-thread CTA per SM
+            if (nblk) {
+                MB_CUDA(allow_dyn_smem(k_blocks<ArsGen4, W, F, 1024>, ArsGen4::kDynSmem));
+                k_blocks<ArsGen4, W, F, 1024><<<grid_for(nblk, 1024, 1), 1024, ArsGen4::kDynSmem, s>>>(
+                    ArsGen4::from(g), B, nblk, out, f);
                 MB_LAUNCH_CHECK();
                 done_blocks = true;
             }
