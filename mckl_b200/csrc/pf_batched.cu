@@ -203,13 +203,21 @@ struct Step {
         if (!init) ls[p] = v;
     }
 
-    // Four pairs of one unit: every load of the unit is issued before any
-    // store, so the loads overlap instead of queueing behind the stores.
-    __device__ __forceinline__ void unit4(const uint32_t (&wr)[4], const uint32_t (&wa)[4],
-        const uint32_t (&pa)[4], const uint32_t (&pb)[4], int lo, int hi, R *v, double *vs) const
-    {
+    // Four pairs of one unit, in two halves: load4 issues every load of the
+    // unit before any store (the loads overlap instead of queueing behind the
+    // stores), move4 moves and weighs the particles and stores them.
+    struct Old {
         R xo[8], lo_[8];
         double xso[8], lso[8];
+    };
+
+    __device__ __forceinline__ void load4(const uint32_t (&pa)[4], const uint32_t (&pb)[4], int lo, int hi,
+        Old &o) const
+    {
+        R(&xo)[8] = o.xo;
+        R(&lo_)[8] = o.lo_;
+        double(&xso)[8] = o.xso;
+        double(&lso)[8] = o.lso;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             xo[2 * j] = xo[2 * j + 1] = lo_[2 * j] = lo_[2 * j + 1] = R(0);
@@ -231,6 +239,15 @@ struct Step {
                 }
             }
         }
+    }
+
+    __device__ __forceinline__ void move4(const uint32_t (&wr)[4], const uint32_t (&wa)[4],
+        const uint32_t (&pa)[4], const uint32_t (&pb)[4], int lo, int hi, const Old &o, R *v, double *vs) const
+    {
+        const R(&xo)[8] = o.xo;
+        const R(&lo_)[8] = o.lo_;
+        const double(&xso)[8] = o.xso;
+        const double(&lso)[8] = o.lso;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             if (j >= lo && j < hi) {
@@ -411,6 +428,51 @@ struct NoiseLayout {
         }
     }
 
+    // The particle slots of unit u at step t (pairs j in [lo, hi) move
+    // particles pa[j], pb[j]) and where its words come from (*src: the radius
+    // block of a full-chunk unit, the radius word of a tail unit); words()
+    // then generates them (decode() in two halves).
+    __device__ __forceinline__ void slots(int t, uint32_t u, uint32_t (&pa)[4], uint32_t (&pb)[4], int *lo_out,
+        int *hi_out, uint64_t *src) const
+    {
+        const uint64_t P = static_cast<uint64_t>(t) * per_step;
+        if (u < m * kUnits) {
+            const uint32_t c32 = u / 129u;
+            const uint64_t c = c32, g = u - c32 * 129u;
+            const uint64_t base = P + c * 1024;
+            *src = (base >> 2) + g;
+            const int i0 = static_cast<int>(4 * g) - static_cast<int>(base & 3);
+            *lo_out = i0 < 0 ? -i0 : 0;
+            *hi_out = i0 + 4 > 512 ? 512 - i0 : 4;
+            const uint32_t q = static_cast<uint32_t>(c * 1024) + static_cast<uint32_t>(i0);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                pa[j] = q + j;  // only [lo, hi) are used
+                pb[j] = q + j + 512;
+            }
+        } else {
+            const uint64_t i = u - m * kUnits;
+            *src = P + m * 1024 + i;
+            pa[0] = static_cast<uint32_t>(m * 1024 + i);
+            pb[0] = static_cast<uint32_t>(m * 1024 + nu_tail + i);
+            *lo_out = 0;
+            *hi_out = 1;
+        }
+    }
+
+    __device__ __forceinline__ void words(const PhiloxGen &gm, uint32_t u, uint64_t src, uint32_t (&wr)[4],
+        uint32_t (&wa)[4]) const
+    {
+        if (u < m * kUnits) {
+            gm.block(Ctr{{src + 1, 0, 0, 0}}, wr);
+            gm.block(Ctr{{src + 129, 0, 0, 0}}, wa);
+        } else {
+            WordCache wc{~0ull, {0, 0, 0, 0}};
+            wr[0] = word_at(gm, src, wc);
+            wa[0] = word_at(gm, src + nu_tail, wc);
+        }
+    }
+
     // the two words of the odd last particle (N odd)
     __device__ __forceinline__ void odd_words(const PhiloxGen &gm, int t, uint32_t *w0, uint32_t *w1) const
     {
@@ -524,8 +586,15 @@ struct FilterRun {
             double vs[8];
             int lo, hi;
             uint32_t wr[4], wa[4], pa[4], pb[4];
-            lay.decode(gm, t, u, wr, wa, pa, pb, &lo, &hi);
-            st.unit4(wr, wa, pa, pb, lo, hi, v, vs);
+            uint64_t src;
+            typename Step<R, SHADOW>::Old old;
+            // the words first, then the loads: issuing the loads before the
+            // generator keeps 16 loaded values live across it, which spills
+            // at the 64-register budget of the resident shapes
+            lay.slots(t, u, pa, pb, &lo, &hi, &src);
+            lay.words(gm, u, src, wr, wa);
+            st.load4(pa, pb, lo, hi, old);
+            st.move4(wr, wa, pa, pb, lo, hi, old, v, vs);
             if (t > 0) {
                 acc.add(v, 2 * lo, 2 * hi);
                 if constexpr (SHADOW) accs.add(vs, 2 * lo, 2 * hi);
@@ -1053,10 +1122,14 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_adjoint(const BatchedFilter *
 // W_{t-1}^j f(xi_t^i | x_{t-1}^j) over the weighted cloud at t - 1 (before its
 // resampling).  The J_k are K = 2 steps of an independent Metropolis-Hastings
 // chain started at the particle's own ancestor (Dau and Chopin 2022, "On
-// backward smoothing algorithms"), the proposal being the ancestor of a
-// uniformly drawn slot: q(j) = rep_j / N, rep_j the copies of j after the
-// resampling (1 without one), so the acceptance ratio is
-//   W_j' f(xi | x_j') rep_J / (W_J f(xi | x_J) rep_j').
+// backward smoothing algorithms").  Its proposal is an even mixture of the
+// ancestor of a uniformly drawn slot and a uniformly drawn particle,
+// q(j) = (rep_j + 1) / 2N with rep_j the copies of j after the resampling
+// (1 without one): drawn in O(1), and positive wherever the target is (the
+// ancestors alone would never propose a particle the resampling dropped, and
+// the chain would sample the backward kernel restricted to the survivors).
+// The acceptance ratio is
+//   W_j' f(xi | x_j') (rep_J + 1) / (W_J f(xi | x_J) (rep_j' + 1)).
 // The estimate is sum_i W_T^i tau_T^i.  Additive terms, theta = (phi, sx, sy):
 //   transition  d = x_t - phi x_{t-1}:  (d x_{t-1} / sx^2, -1/sx + d^2 / sx^3, 0)
 //   observation r = y_t - x_t:           (0, 0, -1/sy + r^2 / sy^3)
@@ -1064,7 +1137,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_adjoint(const BatchedFilter *
 //               v = x_0^2 / sd0^2 - 1:   (v phi / (1 - phi^2), v / sx, 0)
 // The backward draws use Philox4x32 with the filter's resampling key, its
 // second word xor 0x9E3779B9, counter (i, t): one block per particle and
-// step (slot index and acceptance uniform of each of the two moves).
+// step (proposal index in [0, 2N) and acceptance uniform of each move).
 // ---------------------------------------------------------------------------
 struct ScoreArgs {
     uint64_t nmax;
@@ -1141,11 +1214,13 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_score(const BatchedFilter *fi
                 double a0 = 0.0, a1 = 0.0, a2 = 0.0;
 #pragma unroll
                 for (int m = 0; m < 2; ++m) {
-                    const uint32_t k = static_cast<uint32_t>((static_cast<uint64_t>(wd[2 * m]) * N32) >> 32);
-                    const uint32_t jp = anc[k];
+                    // k in [0, 2N): the ancestor of slot k, or particle k - N
+                    const uint32_t k = static_cast<uint32_t>((static_cast<uint64_t>(wd[2 * m]) * (2ull * N32)) >> 32);
+                    const uint32_t jp = k < N32 ? anc[k] : k - N32;
                     const double dp = xi - phi * xprev[jp];
                     // log of the acceptance ratio
-                    const double lr = (dJ * dJ - dp * dp) * hsx2 + log(W[jp] * rep[J]) - log(W[J] * rep[jp]);
+                    const double lr = (dJ * dJ - dp * dp) * hsx2 + log(W[jp] * (rep[J] + 1.0)) -
+                                      log(W[J] * (rep[jp] + 1.0));
                     const double u = (static_cast<double>(wd[2 * m + 1]) + 0.5) * 0x1p-32;
                     if (log(u) < lr) {
                         J = jp;
