@@ -258,7 +258,7 @@ __device__ __forceinline__ bool gamma_n_accept(const GammaParam<R> &k, R u, R w,
 
 // GammaDistribution::generate_{t,w,n,e} (:350-459), the scalar fallback.
 template <typename R, int ALG, class SW>
-__device__ __noinline__ R gamma_scalar(const GammaParam<R> &k, SW &sw, uint64_t &pos)
+__device__ R gamma_scalar(const GammaParam<R> &k, SW &sw, uint64_t &pos)
 {
     using O = GOps<R>;
     const R d = k.d, c = k.c;
@@ -352,8 +352,7 @@ __device__ bool gamma_attempt(const GammaParam<R> &k, SW &sw, uint64_t pos, R *o
 // `left` outputs in attempt order, which is what the sequential loop of
 // gamma_scalar produces.  Returns the words consumed (all lanes agree).
 template <typename R, int ALG, class SW>
-__device__ __noinline__ uint64_t gamma_scalar_warp(const GammaParam<R> &k, SW &sw, uint64_t pos, uint64_t left,
-    R *o)
+__device__ uint64_t gamma_scalar_warp(const GammaParam<R> &k, SW &sw, uint64_t pos, uint64_t left, R *o)
 {
     constexpr uint64_t WA = GammaAttemptWords<ALG>::value;
     const uint32_t lane = threadIdx.x & 31;
@@ -388,8 +387,7 @@ __device__ __noinline__ uint64_t gamma_scalar_warp(const GammaParam<R> &k, SW &s
 // is then drawn by lane 0 with the sequential loop from its (now known)
 // start.  Returns the position after the last value (all lanes agree).
 template <typename R, class G, class SW>
-__device__ __noinline__ uint64_t gamma_scalar_n_warp(const GammaParam<R> &k, SW &sw, uint64_t pos, uint64_t left,
-    R *o)
+__device__ uint64_t gamma_scalar_n_warp(const GammaParam<R> &k, SW &sw, uint64_t pos, uint64_t left, R *o)
 {
     using O = GOps<R>;
     const uint32_t lane = threadIdx.x & 31;
@@ -426,62 +424,6 @@ __device__ __noinline__ uint64_t gamma_scalar_n_warp(const GammaParam<R> &k, SW 
         }
     }
     return pos;
-}
-
-// The redraws of algorithm N on one warp (a rare, cold path, kept out of line
-// so the chunk loop stays small): the scalar normals after the batch words
-// form one sequence z_0, z_1, ... (pair j: words 2j, 2j + 1; z_2j = r cos,
-// z_2j+1 = r sin, the second returned from the cache); the q-th redrawn
-// element takes the q-th z with 1 + c z > 0.  The warp evaluates 64 z at a
-// time and assigns them by ballot ranks into lw / lv; *sh_pos receives the
-// words consumed.
-template <typename R, class G, typename W>
-__device__ __noinline__ void gamma_redraw_warp(const G &g, const Ctr &B, uint32_t off, uint64_t sp0, uint32_t nred,
-    R c, R *lw, R *lv, uint64_t *sh_pos)
-{
-    using O = GOps<R>;
-    const int lane = threadIdx.x;
-    const unsigned lt = (1u << lane) - 1u;
-    ScalarWords<G, W> sw{&g, B, off};
-    uint32_t done = 0;
-    uint64_t used = 0;  // normals consumed
-    for (uint64_t pb = 0; done < nred; pb += 32) {
-        const uint64_t j = pb + lane;
-        uint64_t k = sp0 + 2 * j;
-        ScalarNormal<R> rn;
-        const R z0 = rn(sw, k), z1 = rn(sw, k);
-        const R v0 = O::add(static_cast<R>(1), O::mul(c, z0));
-        const R v1 = O::add(static_cast<R>(1), O::mul(c, z1));
-        const bool a0 = v0 > 0, a1 = v1 > 0;
-        const unsigned m0 = __ballot_sync(0xffffffffu, a0), m1 = __ballot_sync(0xffffffffu, a1);
-        const uint32_t before = __popc(m0 & lt) + __popc(m1 & lt);
-        const uint32_t r0 = before, r1 = before + (a0 ? 1u : 0u);
-        const uint32_t need = nred - done;
-        if (a0 && r0 < need) {
-            lw[done + r0] = z0;
-            lv[done + r0] = v0;
-        }
-        if (a1 && r1 < need) {
-            lw[done + r1] = z1;
-            lv[done + r1] = v1;
-        }
-        const uint32_t tot = __popc(m0) + __popc(m1);
-        if (tot >= need) {
-            // the need-th accepted normal is the last one consumed
-            const bool last0 = a0 && r0 == need - 1, last1 = a1 && r1 == need - 1;
-            const unsigned ml = __ballot_sync(0xffffffffu, last0 || last1);
-            const int src = __ffs(ml) - 1;
-            const uint32_t idx = last0 ? 2u * lane : 2u * lane + 1u;
-            const uint32_t li = __shfl_sync(0xffffffffu, idx, src);
-            used = 2 * pb + li + 1;
-            done = nred;
-        } else {
-            done += tot;
-        }
-    }
-    // consumed words: two per started pair (a cached second value is dropped
-    // with the chunk's normal generator)
-    if (lane == 0) *sh_pos = 2 * ((used + 1) / 2);
 }
 
 template <typename R>
@@ -625,7 +567,56 @@ __device__ uint32_t gamma_chunk(const G &g, const GammaParam<R> &k, const Ctr &B
         }
         if (nred) {
             __syncthreads();
-            if (threadIdx.x < 32) gamma_redraw_warp<R, G, W>(g, B, off, pos + nw, nred, c, lw, lv, sh_pos);
+            if (threadIdx.x < 32) {
+                // The scalar normals after the batch words form one sequence
+                // z_0, z_1, ... (pair j: words 2j, 2j + 1; z_2j = r cos, z_2j+1
+                // = r sin, the second returned from the cache); the q-th
+                // redrawn element takes the q-th z with 1 + c z > 0.  A warp
+                // evaluates 64 z at a time and assigns them by ballot ranks.
+                const int lane = threadIdx.x;
+                const unsigned lt = (1u << lane) - 1u;
+                ScalarWords<G, W> sw{&g, B, off};
+                const uint64_t sp0 = pos + nw;
+                uint32_t done = 0;
+                uint64_t used = 0;  // normals consumed
+                for (uint64_t pb = 0; done < nred; pb += 32) {
+                    const uint64_t j = pb + lane;
+                    uint64_t k = sp0 + 2 * j;
+                    ScalarNormal<R> rn;
+                    const R z0 = rn(sw, k), z1 = rn(sw, k);
+                    const R v0 = O::add(static_cast<R>(1), O::mul(c, z0));
+                    const R v1 = O::add(static_cast<R>(1), O::mul(c, z1));
+                    const bool a0 = v0 > 0, a1 = v1 > 0;
+                    const unsigned m0 = __ballot_sync(0xffffffffu, a0), m1 = __ballot_sync(0xffffffffu, a1);
+                    const uint32_t before = __popc(m0 & lt) + __popc(m1 & lt);
+                    const uint32_t r0 = before, r1 = before + (a0 ? 1u : 0u);
+                    const uint32_t need = nred - done;
+                    if (a0 && r0 < need) {
+                        lw[done + r0] = z0;
+                        lv[done + r0] = v0;
+                    }
+                    if (a1 && r1 < need) {
+                        lw[done + r1] = z1;
+                        lv[done + r1] = v1;
+                    }
+                    const uint32_t tot = __popc(m0) + __popc(m1);
+                    if (tot >= need) {
+                        // the need-th accepted normal is the last one consumed
+                        const bool last0 = a0 && r0 == need - 1, last1 = a1 && r1 == need - 1;
+                        const unsigned ml = __ballot_sync(0xffffffffu, last0 || last1);
+                        const int src = __ffs(ml) - 1;
+                        const uint32_t idx = last0 ? 2u * lane : 2u * lane + 1u;
+                        const uint32_t li = __shfl_sync(0xffffffffu, idx, src);
+                        used = 2 * pb + li + 1;
+                        done = nred;
+                    } else {
+                        done += tot;
+                    }
+                }
+                // consumed words: two per started pair (a cached second value
+                // is dropped with the chunk's normal generator)
+                if (lane == 0) *sh_pos = 2 * ((used + 1) / 2);
+            }
             __syncthreads();
 #pragma unroll
             for (int j = 0; j < EPT; ++j) {
