@@ -1187,15 +1187,16 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_score(const BatchedFilter *fi
             const double x0 = run.xc[p];
             const double v = x0 * x0 * isd02 - 1.0;
             xbuf[0][p] = x0;
-            W[p] = 1.0 / static_cast<double>(N);
-            rep[p] = 1;
-            anc[p] = static_cast<uint32_t>(p);
+            W[p] = 1.0;
             taub[0][p] = v * phi / q0;
             taub[0][nm + p] = v / sx;
             taub[0][2 * nm + p] = 0.0;
         }
         __syncthreads();
         int cur = 0;
+        // whether the cloud at t - 1 was resampled: otherwise its slots are
+        // their own parents (anc = identity, rep = 1) and the arrays are not read
+        bool resampled = false;
         for (int t = 1; t <= T; ++t) {
             double *xprev = xbuf[(t - 1) & 1], *xnow = xbuf[t & 1];
             run.rec_x = xnow;  // the step records its cloud before resampling
@@ -1209,18 +1210,18 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_score(const BatchedFilter *fi
                 const double xi = xnow[i];
                 uint32_t wd[4];
                 gb.block(Ctr{{i, static_cast<uint64_t>(t), 0, 0}}, wd);
-                uint32_t J = anc[i];
+                uint32_t J = resampled ? anc[i] : static_cast<uint32_t>(i);
                 double dJ = xi - phi * xprev[J];
                 double a0 = 0.0, a1 = 0.0, a2 = 0.0;
 #pragma unroll
                 for (int m = 0; m < 2; ++m) {
                     // k in [0, 2N): the ancestor of slot k, or particle k - N
                     const uint32_t k = static_cast<uint32_t>((static_cast<uint64_t>(wd[2 * m]) * (2ull * N32)) >> 32);
-                    const uint32_t jp = k < N32 ? anc[k] : k - N32;
+                    const uint32_t jp = k < N32 ? (resampled ? anc[k] : k) : k - N32;
                     const double dp = xi - phi * xprev[jp];
                     // log of the acceptance ratio
-                    const double lr = (dJ * dJ - dp * dp) * hsx2 + log(W[jp] * (rep[J] + 1.0)) -
-                                      log(W[J] * (rep[jp] + 1.0));
+                    const double rJ = resampled ? rep[J] + 1.0 : 2.0, rp = resampled ? rep[jp] + 1.0 : 2.0;
+                    const double lr = (dJ * dJ - dp * dp) * hsx2 + log(W[jp] * rJ) - log(W[J] * rp);
                     const double u = (static_cast<double>(wd[2 * m + 1]) + 0.5) * 0x1p-32;
                     if (log(u) < lr) {
                         J = jp;
@@ -1238,23 +1239,18 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_score(const BatchedFilter *fi
             }
             cur ^= 1;
             __syncthreads();
-            // the cloud at t for the next step: normalised weights (the
-            // log-weights are left as they were before the resampling) and,
-            // when it was resampled, the parents of the slots
-            double mx = -INFINITY;
-            for (uint64_t p = threadIdx.x; p < N; p += THREADS) mx = fmax(mx, run.st.l[p]);
-            mx = block_max(mx, shd);
-            double ssum = 0.0;
+            // the cloud at t for the next step: weights relative to the
+            // step's largest (the step leaves its log-weights as they were
+            // before the resampling and their maximum in lshift; the ratios
+            // above need no normalisation) and, when it was resampled, the
+            // parents of the slots
+            const double mx = run.st.lshift;
             for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
-                const double e = exp(run.st.l[p] - mx);
-                W[p] = e;
-                ssum += e;
-                anc[p] = static_cast<uint32_t>(p);
+                W[p] = exp(run.st.l[p] - mx);
+                if (res) anc[p] = static_cast<uint32_t>(p);
             }
-            ssum = block_sum(ssum, shd);
-            const double inv = 1.0 / ssum;
-            for (uint64_t p = threadIdx.x; p < N; p += THREADS) W[p] *= inv;
             __syncthreads();
+            resampled = res;
             if (res) {
                 // slot-preserving placement: parent p keeps slot p when it
                 // has copies and fills the empties ep[sS_p .. sS_{p+1})
@@ -1270,22 +1266,25 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_score(const BatchedFilter *fi
                     const uint32_t b = run.sS[p], e = p + 1 < N ? run.sS[p + 1] : ne;
                     rep[p] = (anc[p] == p ? 1u : 0u) + (e - b);
                 }
-            } else {
-                for (uint64_t p = threadIdx.x; p < N; p += THREADS) rep[p] = 1;
+                __syncthreads();
             }
-            __syncthreads();
         }
-        // the estimate: sum_i W_T^i tau_T^i
-        double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+        // the estimate: sum_i W_T^i tau_T^i / sum_i W_T^i
+        double g0 = 0.0, g1 = 0.0, g2 = 0.0, gw = 0.0;
         const double *tT = taub[cur];
         for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
             g0 += W[p] * tT[p];
             g1 += W[p] * tT[nm + p];
             g2 += W[p] * tT[2 * nm + p];
+            gw += W[p];
         }
         g0 = block_sum(g0, shd);
         g1 = block_sum(g1, shd);
         g2 = block_sum(g2, shd);
+        gw = block_sum(gw, shd);
+        g0 /= gw;
+        g1 /= gw;
+        g2 /= gw;
         if (threadIdx.x == 0) {
             loglik[f] = run.ll_sum;
             nresampled[f] = static_cast<uint32_t>(run.events);
