@@ -7,8 +7,9 @@
 // does with rng_set[0] (smp/backend_seq.hpp:60-64); resampling uses the
 // particle's own engine (core/particle.hpp:364).  Every piece is the
 // bit-faithful kernel of its reference function; the loop itself runs on the
-// host and synchronizes once per step to read the ESS that decides the
-// resampling, as the reference's loop does.
+// host and waits once per step for the ESS that decides the resampling, as
+// the reference's loop does, with the next step's model noise (which does not
+// depend on the decision) already queued behind the read-back.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -51,6 +52,19 @@ unsigned grid_of(uint64_t n)
 
 // scan ties of the calling thread's last plain-filter run
 thread_local uint64_t g_last_ties = 0;
+
+// Page-locked landing place of the per-step (ESS, log normaliser) pair and an
+// event marking its copy, one per host thread (allocated once).
+struct StepReadback {
+    double *h = nullptr;
+    cudaEvent_t ev = nullptr;
+    ~StepReadback()
+    {
+        if (ev) cudaEventDestroy(ev);
+        if (h) cudaFreeHost(h);
+    }
+};
+thread_local StepReadback g_rb;
 
 }  // namespace
 
@@ -103,23 +117,37 @@ extern "C" int mckl_b200_pf_ar1_plain_f64(size_t N, size_t T, const double *y, d
     MB_CUDA(cudaMemsetAsync(ties, 0, sizeof(unsigned long long), s));
     k_fill<<<grid_of(N), 256, 0, s>>>(N, W_dev, equal);
     MB_LAUNCH_CHECK();
+    if (!g_rb.h) {
+        MB_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&g_rb.h), 2 * sizeof(double), cudaHostAllocDefault));
+        MB_CUDA(cudaEventCreateWithFlags(&g_rb.ev, cudaEventDisableTiming));
+    }
     double ess = static_cast<double>(N), ll_sum = 0.0;
     for (size_t it = 0; it <= T; ++it) {
         if (it == 0) {
             int rc = mckl_b200_normal_f64(&em, N, x_dev, 0.0, sd0, stream);
             if (rc != MCKL_B200_OK) return rc;
+            if (T > 0) {
+                rc = mckl_b200_normal_f64(&em, N, eps, 0.0, 1.0, stream);  // the noise of step 1
+                if (rc != MCKL_B200_OK) return rc;
+            }
         } else {
-            int rc = mckl_b200_normal_f64(&em, N, eps, 0.0, 1.0, stream);
-            if (rc != MCKL_B200_OK) return rc;
+            // eps holds this step's noise (drawn during the previous step's
+            // round trip): the model stream does not depend on the decisions
             k_ar1_propagate<<<grid_of(N), 256, 0, s>>>(N, x_dev, eps, y[it], phi, sx, lconst, hinv, ll);
             MB_LAUNCH_CHECK();
-            rc = weight_normalize_dev(N, W_dev, ll, 1, wscr, wres, s);
+            int rc = weight_normalize_dev(N, W_dev, ll, 1, wscr, wres, s);
             if (rc != MCKL_B200_OK) return rc;
-            double h[2];
-            MB_CUDA(cudaMemcpyAsync(h, wres, sizeof(h), cudaMemcpyDeviceToHost, s));
-            MB_CUDA(cudaStreamSynchronize(s));
-            ess = h[0];
-            ll_sum += h[1];
+            MB_CUDA(cudaMemcpyAsync(g_rb.h, wres, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+            MB_CUDA(cudaEventRecord(g_rb.ev, s));
+            // the next step's noise keeps the device busy while the host
+            // reads the ESS and decides
+            if (it < T) {
+                rc = mckl_b200_normal_f64(&em, N, eps, 0.0, 1.0, stream);
+                if (rc != MCKL_B200_OK) return rc;
+            }
+            MB_CUDA(cudaEventSynchronize(g_rb.ev));
+            ess = g_rb.h[0];
+            ll_sum += g_rb.h[1];
         }
         if (ess_hist) ess_hist[it] = ess;
         if (resampled) resampled[it] = 0;
