@@ -45,6 +45,61 @@ __global__ void k_ar1_propagate(uint64_t n, double *x, const double *eps, double
     }
 }
 
+// the same move with y_t read from the device (t = *t_dev), for the captured step
+__global__ void k_ar1_propagate_dev(uint64_t n, double *x, const double *eps, const double *y, const int *t_dev,
+    double phi, double sx, double lconst, double hinv, double *ll)
+{
+    const double yt = y[*t_dev];
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const double a = __dmul_rn(phi, x[i]);
+        const double b = __dmul_rn(sx, eps[i]);
+        const double xn = __dadd_rn(a, b);
+        x[i] = xn;
+        const double r = __dsub_rn(yt, xn);
+        ll[i] = __dsub_rn(lconst, __dmul_rn(__dmul_rn(r, r), hinv));
+    }
+}
+
+__global__ void k_step_inc(int *t_dev)
+{
+    *t_dev += 1;
+}
+
+// Capture the work `fn` enqueues (on a private stream) into an instantiated graph.
+template <class Fn>
+int capture(cudaGraphExec_t *exec, Fn &&fn)
+{
+    cudaStream_t cap;
+    MB_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaError_t ce = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (ce != cudaSuccess) {
+        cudaStreamDestroy(cap);
+        MB_CUDA(ce);
+    }
+    const int rc = fn(cap);
+    cudaGraph_t g = nullptr;
+    ce = cudaStreamEndCapture(cap, &g);
+    cudaStreamDestroy(cap);
+    if (rc != MCKL_B200_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    MB_CUDA(ce);
+    ce = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    MB_CUDA(ce);
+    return MCKL_B200_OK;
+}
+
+struct GraphExec {
+    cudaGraphExec_t e = nullptr;
+    ~GraphExec()
+    {
+        if (e) cudaGraphExecDestroy(e);
+    }
+};
+
 unsigned grid_of(uint64_t n)
 {
     return static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 148 * 16)));
@@ -84,7 +139,7 @@ extern "C" int mckl_b200_pf_ar1_plain_f64(size_t N, size_t T, const double *y, d
     cudaStream_t s = as_stream(stream);
     // work buffers: eps, ll, rep, idx, result words
     const size_t wsz = weight_scratch_bytes(N), rsz = resample_scratch_bytes(N, N), isz = rep_index_scratch_bytes(N, N);
-    const size_t buf = 4 * align256(N * sizeof(double)) + 512;
+    const size_t buf = 4 * align256(N * sizeof(double)) + 512 + align256((T + 1) * sizeof(double));
     char *base = static_cast<char *>(scratch(5, buf + wsz + rsz + isz, s));
     if (!base) {
         set_error("particle filter scratch allocation failed");
@@ -97,6 +152,8 @@ extern "C" int mckl_b200_pf_ar1_plain_f64(size_t N, size_t T, const double *y, d
     double *wres = reinterpret_cast<double *>(base + 4 * align256(N * 8));
     int *err = reinterpret_cast<int *>(base + 4 * align256(N * 8) + 256);
     unsigned long long *ties = reinterpret_cast<unsigned long long *>(base + 4 * align256(N * 8) + 384);
+    int *t_dev = reinterpret_cast<int *>(base + 4 * align256(N * 8) + 448);
+    double *y_dev = reinterpret_cast<double *>(base + 4 * align256(N * 8) + 512);
     void *wscr = base + buf;
     void *rscr = base + buf + wsz;
     void *iscr = base + buf + wsz + rsz;
@@ -122,49 +179,121 @@ extern "C" int mckl_b200_pf_ar1_plain_f64(size_t N, size_t T, const double *y, d
         MB_CUDA(cudaEventCreateWithFlags(&g_rb.ev, cudaEventDisableTiming));
     }
     double ess = static_cast<double>(N), ll_sum = 0.0;
-    for (size_t it = 0; it <= T; ++it) {
-        if (it == 0) {
-            int rc = mckl_b200_normal_f64(&em, N, x_dev, 0.0, sd0, stream);
-            if (rc != MCKL_B200_OK) return rc;
-            if (T > 0) {
-                rc = mckl_b200_normal_f64(&em, N, eps, 0.0, 1.0, stream);  // the noise of step 1
-                if (rc != MCKL_B200_OK) return rc;
-            }
-        } else {
-            // eps holds this step's noise (drawn during the previous step's
-            // round trip): the model stream does not depend on the decisions
-            k_ar1_propagate<<<grid_of(N), 256, 0, s>>>(N, x_dev, eps, y[it], phi, sx, lconst, hinv, ll);
+    if (scheme <= 2) {
+        // Schemes without residuals: the engine-independent work of a step is
+        // two CUDA graphs built once per call -- A: next step, move, weight
+        // normalisation, read-back of (ESS, log normaliser); B: the exact
+        // cumulative fold, replication counts, rep -> index, select and equal
+        // weights -- so a step costs a handful of host calls.  The noise and
+        // the resampling uniforms (the engines' positions) are launched as
+        // before.
+        static const int seq_of[3] = {0, 1, 2};
+        ResampleScratch rs = resample_scratch_carve(rscr, N, N);
+        MB_CUDA(cudaMemcpyAsync(y_dev, y, (T + 1) * sizeof(double), cudaMemcpyHostToDevice, s));
+        MB_CUDA(cudaMemsetAsync(t_dev, 0, sizeof(int), s));
+        GraphExec ga, gb;
+        int rc = capture(&ga.e, [&](cudaStream_t c) {
+            k_step_inc<<<1, 1, 0, c>>>(t_dev);
             MB_LAUNCH_CHECK();
-            int rc = weight_normalize_dev(N, W_dev, ll, 1, wscr, wres, s);
-            if (rc != MCKL_B200_OK) return rc;
-            MB_CUDA(cudaMemcpyAsync(g_rb.h, wres, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
-            MB_CUDA(cudaEventRecord(g_rb.ev, s));
-            // the next step's noise keeps the device busy while the host
-            // reads the ESS and decides
-            if (it < T) {
-                rc = mckl_b200_normal_f64(&em, N, eps, 0.0, 1.0, stream);
+            k_ar1_propagate_dev<<<grid_of(N), 256, 0, c>>>(N, x_dev, eps, y_dev, t_dev, phi, sx, lconst, hinv, ll);
+            MB_LAUNCH_CHECK();
+            int r = weight_normalize_dev(N, W_dev, ll, 1, wscr, wres, c);
+            if (r != MCKL_B200_OK) return r;
+            MB_CUDA(cudaMemcpyAsync(g_rb.h, wres, 2 * sizeof(double), cudaMemcpyDeviceToHost, c));
+            return MCKL_B200_OK;
+        });
+        if (rc != MCKL_B200_OK) return rc;
+        rc = capture(&gb.e, [&](cudaStream_t c) {
+            int r = rep_counts_dev(N, N, W_dev, rs.u, rep, rs, c, ties);
+            if (r != MCKL_B200_OK) return r;
+            r = rep_to_index_dev(N, N, rep, idx, iscr, err, c);
+            if (r != MCKL_B200_OK) return r;
+            r = select_dev<double>(N, N, 1, idx, x_dev, x_dev, c);
+            if (r != MCKL_B200_OK) return r;
+            k_fill<<<grid_of(N), 256, 0, c>>>(N, W_dev, equal);
+            MB_LAUNCH_CHECK();
+            return MCKL_B200_OK;
+        });
+        if (rc != MCKL_B200_OK) return rc;
+        for (size_t it = 0; it <= T; ++it) {
+            if (it == 0) {
+                rc = mckl_b200_normal_f64(&em, N, x_dev, 0.0, sd0, stream);
                 if (rc != MCKL_B200_OK) return rc;
+                if (T > 0) {
+                    rc = mckl_b200_normal_f64(&em, N, eps, 0.0, 1.0, stream);
+                    if (rc != MCKL_B200_OK) return rc;
+                }
+            } else {
+                MB_CUDA(cudaGraphLaunch(ga.e, s));
+                count_launch();
+                MB_CUDA(cudaEventRecord(g_rb.ev, s));
+                if (it < T) {
+                    rc = mckl_b200_normal_f64(&em, N, eps, 0.0, 1.0, stream);
+                    if (rc != MCKL_B200_OK) return rc;
+                }
+                MB_CUDA(cudaEventSynchronize(g_rb.ev));
+                ess = g_rb.h[0];
+                ll_sum += g_rb.h[1];
             }
-            MB_CUDA(cudaEventSynchronize(g_rb.ev));
-            ess = g_rb.h[0];
-            ll_sum += g_rb.h[1];
+            if (ess_hist) ess_hist[it] = ess;
+            if (resampled) resampled[it] = 0;
+            if (ess < static_cast<double>(N) * threshold) {
+                rc = u01_sequence_dev(seq_of[scheme], er, N, rs.u, rs.tmp, rs.fs, s);
+                if (rc != MCKL_B200_OK) return rc;
+                MB_CUDA(cudaGraphLaunch(gb.e, s));
+                count_launch();
+                if (anc_dev) {
+                    MB_CUDA(cudaMemcpyAsync(anc_dev + it * N, idx, N * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+                }
+                ess = static_cast<double>(N);
+                if (resampled) resampled[it] = 1;
+            }
         }
-        if (ess_hist) ess_hist[it] = ess;
-        if (resampled) resampled[it] = 0;
-        if (ess < static_cast<double>(N) * threshold) {
-            int rc = resample_dev(scheme, N, N, er, W_dev, rep, rscr, s, ties);
-            if (rc != MCKL_B200_OK) return rc;
-            rc = rep_to_index_dev(N, N, rep, idx, iscr, err, s);
-            if (rc != MCKL_B200_OK) return rc;
-            if (anc_dev) {
-                MB_CUDA(cudaMemcpyAsync(anc_dev + it * N, idx, N * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+    } else {
+        for (size_t it = 0; it <= T; ++it) {
+            if (it == 0) {
+                int rc = mckl_b200_normal_f64(&em, N, x_dev, 0.0, sd0, stream);
+                if (rc != MCKL_B200_OK) return rc;
+                if (T > 0) {
+                    rc = mckl_b200_normal_f64(&em, N, eps, 0.0, 1.0, stream);  // the noise of step 1
+                    if (rc != MCKL_B200_OK) return rc;
+                }
+            } else {
+                // eps holds this step's noise (drawn during the previous step's
+                // round trip): the model stream does not depend on the decisions
+                k_ar1_propagate<<<grid_of(N), 256, 0, s>>>(N, x_dev, eps, y[it], phi, sx, lconst, hinv, ll);
+                MB_LAUNCH_CHECK();
+                int rc = weight_normalize_dev(N, W_dev, ll, 1, wscr, wres, s);
+                if (rc != MCKL_B200_OK) return rc;
+                MB_CUDA(cudaMemcpyAsync(g_rb.h, wres, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+                MB_CUDA(cudaEventRecord(g_rb.ev, s));
+                // the next step's noise keeps the device busy while the host
+                // reads the ESS and decides
+                if (it < T) {
+                    rc = mckl_b200_normal_f64(&em, N, eps, 0.0, 1.0, stream);
+                    if (rc != MCKL_B200_OK) return rc;
+                }
+                MB_CUDA(cudaEventSynchronize(g_rb.ev));
+                ess = g_rb.h[0];
+                ll_sum += g_rb.h[1];
             }
-            rc = select_dev<double>(N, N, 1, idx, x_dev, x_dev, s);
-            if (rc != MCKL_B200_OK) return rc;
-            k_fill<<<grid_of(N), 256, 0, s>>>(N, W_dev, equal);
-            MB_LAUNCH_CHECK();
-            ess = static_cast<double>(N);
-            if (resampled) resampled[it] = 1;
+            if (ess_hist) ess_hist[it] = ess;
+            if (resampled) resampled[it] = 0;
+            if (ess < static_cast<double>(N) * threshold) {
+                int rc = resample_dev(scheme, N, N, er, W_dev, rep, rscr, s, ties);
+                if (rc != MCKL_B200_OK) return rc;
+                rc = rep_to_index_dev(N, N, rep, idx, iscr, err, s);
+                if (rc != MCKL_B200_OK) return rc;
+                if (anc_dev) {
+                    MB_CUDA(cudaMemcpyAsync(anc_dev + it * N, idx, N * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+                }
+                rc = select_dev<double>(N, N, 1, idx, x_dev, x_dev, s);
+                if (rc != MCKL_B200_OK) return rc;
+                k_fill<<<grid_of(N), 256, 0, s>>>(N, W_dev, equal);
+                MB_LAUNCH_CHECK();
+                ess = static_cast<double>(N);
+                if (resampled) resampled[it] = 1;
+            }
         }
     }
     int h = 0;

@@ -457,6 +457,32 @@ int resample_dev(int scheme, uint64_t N, uint64_t M, mckl_b200_engine_t &e, cons
     return MCKL_B200_OK;
 }
 
+ResampleScratch resample_scratch_carve(void *scratch_base, uint64_t N, uint64_t M)
+{
+    const uint64_t L = std::max<uint64_t>(std::max<uint64_t>(N, M), 1);
+    char *p = static_cast<char *>(scratch_base) + 1024;
+    ResampleScratch r;
+    r.u = reinterpret_cast<double *>(p);
+    r.tmp = reinterpret_cast<double *>(p + align256(L * sizeof(double)));
+    r.fs = fold_scratch_carve(p + 3 * align256(L * sizeof(double)) + align256(L * sizeof(uint64_t)), L);
+    return r;
+}
+
+int rep_counts_dev(uint64_t N, uint64_t M, const double *W, const double *u, uint64_t *rep, ResampleScratch &rs,
+    cudaStream_t s, unsigned long long *ties_dev)
+{
+    if (N <= 1 || M == 0) {
+        k_fill_rep<<<cap_grid(N, 256), 256, 0, s>>>(N, M, rep);
+        MB_LAUNCH_CHECK();
+        return MCKL_B200_OK;
+    }
+    int rc = fold_exact(W, N - 1, 0.0, rs.tmp, rs.fs, s);  // cumulative weights of particles 0..N-2
+    if (rc != MCKL_B200_OK) return rc;
+    k_rep_counts<<<cap_grid(N, 256), 256, 0, s>>>(N, M, rs.tmp, u, rep, ties_dev);
+    MB_LAUNCH_CHECK();
+    return MCKL_B200_OK;
+}
+
 size_t rep_index_scratch_bytes(uint64_t N, uint64_t M)
 {
     const uint64_t tiles = (N + kScanTile - 1) / kScanTile + 1;

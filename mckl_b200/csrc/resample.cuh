@@ -28,6 +28,18 @@ int resample_dev(int scheme, uint64_t N, uint64_t M, mckl_b200_engine_t &e, cons
     void *scratch_base, cudaStream_t s, unsigned long long *ties_dev = nullptr);
 int rep_to_index_dev(uint64_t N, uint64_t M, const uint64_t *rep, uint64_t *idx, void *scratch_base, int *err_dev,
     cudaStream_t s);
+
+// The pieces of resample_dev for the schemes without residuals (0, 1, 2), so
+// a caller can put the engine-independent half in a CUDA graph: the uniforms
+// go to rs.u (u01_sequence_dev with rs.tmp and rs.fs), then rep_counts_dev
+// folds W and counts (no engine, no host synchronisation).
+struct ResampleScratch {
+    double *u, *tmp;
+    FoldScratch fs;
+};
+ResampleScratch resample_scratch_carve(void *scratch_base, uint64_t N, uint64_t M);
+int rep_counts_dev(uint64_t N, uint64_t M, const double *W, const double *u, uint64_t *rep, ResampleScratch &rs,
+    cudaStream_t s, unsigned long long *ties_dev);
 template <typename T>
 int select_dev(uint64_t N, uint64_t M, uint64_t dim, const uint64_t *idx, const T *in, T *out, cudaStream_t s);
 
