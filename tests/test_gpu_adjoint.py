@@ -103,8 +103,11 @@ def test_adjoint_vs_kalman_gradient(env):
     the ancestors drops the dependence of the resampling on theta, so this
     gradient is a biased estimate of the score whatever N is (it drops the
     score of the resampling step); the check is only that it points into the
-    same half-space as the exact score and that the log-likelihood itself is
-    close to Kalman's -- the size of the bias is reported by the benchmark."""
+    same direction as the exact score (cosine above 0.8; 0.94 measured at the
+    differentiated configuration) with the bias below 1.5 times its size (0.95
+    measured), and that the log-likelihood itself is close to Kalman's.  The
+    consistent estimate of the score, and its error against Kalman within its
+    Monte Carlo error, is test_gpu_score's; the benchmark reports both."""
     mb, orc = env
     w = mb.batched_workload(F=8, T=100, seed=5, nmin=1 << 16, nmax=(1 << 16) + 1)
     w["threads"] = 512
@@ -117,4 +120,4 @@ def test_adjoint_vs_kalman_gradient(env):
         assert abs(ll[f] - kll) < 1.0, (f, ll[f], kll)
     cos = float(np.sum(g * kg) / (np.linalg.norm(g) * np.linalg.norm(kg)))
     rel = float(np.linalg.norm(g - kg) / np.linalg.norm(kg))
-    assert cos > 0.5 and rel < 3.0, (cos, rel)
+    assert cos > 0.8 and rel < 1.5, (cos, rel)
