@@ -9,8 +9,8 @@ namespace mckl_b200 {
 
 namespace {
 
-constexpr int kDescThreads = 256;
-constexpr int kPer = kFoldTile / kDescThreads;  // 16 consecutive elements per thread
+constexpr int kDescThreads = 512;
+constexpr int kPer = kFoldTile / kDescThreads;  // 8 consecutive elements per thread
 constexpr int kWalkThreads = 1024;
 constexpr int kWalkPer = kFoldTile / kWalkThreads;  // 4
 constexpr unsigned kSeqStretch = 256;  // elements folded one at a time after two scan rounds of a tile
@@ -28,7 +28,7 @@ __device__ __forceinline__ double ulp_of(double v)
 // A_j is a parallel (tree) sum of s0 + x_0 + ... + x_j; S_j the sequential
 // fold.  Both are sums of nonnegative terms, so |A_j - S_j| <= (j + 1 + D)
 // 2^-53 A_j (first order) with D the depth of A's summation tree (below
-// 100 + T / 1024 here: 16 sequential adds per thread, two CTA scans, the
+// 100 + T / 1024 here: 8 sequential adds per thread, two CTA scans, the
 // tile scan with its carries).  ulp(A) > 2^-53 A, so a margin of
 // 2 (j + 1) + 2 T + 160 ulps of A_j holds S_j with room to spare: when
 // [A_j - margin, A_j + margin] lies inside one binade, S_j certainly does.
@@ -43,10 +43,10 @@ __device__ __forceinline__ int certain_binade(double A, uint64_t j, uint64_t T)
     return e;
 }
 
-// The tile's kPer elements of this thread (zeros past n) and the
-// approximate partial sum before the first of them.
+// The tile's kPer elements of this thread (zeros past n), the approximate
+// partial sum before the first of them and their own sum.
 __device__ __forceinline__ void tile_load(const double *x, uint64_t n, double s0, const double *tpre, uint64_t t,
-    double (&xv)[kPer], double *sh, double *Abefore)
+    double (&xv)[kPer], double *sh, double *Abefore, double *own_sum = nullptr)
 {
     const uint64_t i0 = t * kFoldTile + static_cast<uint64_t>(threadIdx.x) * kPer;
     double own = 0.0;
@@ -58,6 +58,7 @@ __device__ __forceinline__ void tile_load(const double *x, uint64_t n, double s0
     double tot;
     const double ex = block_exclusive_sum(own, sh, &tot);
     *Abefore = __dadd_rn(__dadd_rn(s0, tpre[t]), ex);
+    if (own_sum) *own_sum = own;
 }
 
 // Element j = i0 + k is a RUN element when the binades of S_{j-1} and S_j
@@ -66,9 +67,36 @@ __device__ __forceinline__ void tile_load(const double *x, uint64_t n, double s0
 // is a WINDOW: the walk folds it with a real double add.  Returns, per
 // element, q (0 for windows), the window bit and the certain binade of
 // S_{j-1} (-1: uncertain).
+//
+// Fast case: S_{i0-1} .. S_{i0+kPer-1} all lie in [A_before - m, A_end + m]
+// (the partial sums grow, and A_end = A_before + the thread's own sum is a
+// summation tree of the same depth as the per-element A_j), with m the margin
+// of the last element, the largest.  When that interval lies in one binade,
+// every element's binade is certain and the same, and only its increment
+// remains to be checked.
 __device__ __forceinline__ void classify(const double (&xv)[kPer], uint64_t i0, uint64_t n, uint64_t T, double s0,
-    double Abefore, long long (&q)[kPer], unsigned &win, int (&eprev)[kPer])
+    double Abefore, double own, long long (&q)[kPer], unsigned &win, int (&eprev)[kPer])
 {
+    {
+        const double Aend = __dadd_rn(Abefore, own);
+        const double c = 2.0 * static_cast<double>(i0 + kPer) + 2.0 * static_cast<double>(T) + 160.0;
+        const double lo = __dsub_rn(Abefore, c * ulp_of(Abefore)), hi = __dadd_rn(Aend, c * ulp_of(Aend));
+        const int e = biased_exp(lo);
+        if (lo > 0.0 && e != 0x7ff && biased_exp(hi) == e) {
+            win = 0;
+#pragma unroll
+            for (int k = 0; k < kPer; ++k) {
+                bool ev;
+                q[k] = grid_increment(xv[k], e, ev);  // xv is 0 past n: q = 0, no event
+                eprev[k] = e;
+                if (ev) {
+                    q[k] = 0;
+                    win |= 1u << k;
+                }
+            }
+            return;
+        }
+    }
     int ep;
     if (i0 == 0) {
         ep = (s0 > 0.0 && biased_exp(s0) != 0x7ff) ? biased_exp(s0) : -1;  // s0 itself is exact
@@ -125,10 +153,12 @@ __global__ void __launch_bounds__(1024) k_fold_scan_tiles(const double *tsum, ui
     }
 }
 
-// 3. per tile: the sum of the run increments and the number of windows; and
-// the tile descriptor of the event-loop walk (the fallback)
+// 3. per tile: the sum of the run increments and the number of windows, the
+// tile's window list (when it fits), and the tile descriptor of the
+// event-loop walk (the fallback)
 __global__ void __launch_bounds__(kDescThreads) k_fold_count(const double *x, uint64_t n, double s0,
-    const double *tsum, const double *tpre, uint64_t T, long long *tq, unsigned *tw, FoldDesc *desc, int *elast)
+    const double *tsum, const double *tpre, uint64_t T, long long *tq, unsigned *tw, FoldDesc *desc, int *elast,
+    FoldLocal loc)
 {
     __shared__ double shd[33];
     __shared__ long long shl[33];
@@ -136,19 +166,18 @@ __global__ void __launch_bounds__(kDescThreads) k_fold_count(const double *x, ui
     const uint64_t t = blockIdx.x;
     const uint64_t base = t * kFoldTile;
     const uint64_t i0 = base + static_cast<uint64_t>(threadIdx.x) * kPer;
-    double xv[kPer], Ab;
-    tile_load(x, n, s0, tpre, t, xv, shd, &Ab);
+    double xv[kPer], Ab, own;
+    tile_load(x, n, s0, tpre, t, xv, shd, &Ab, &own);
     long long q[kPer];
     unsigned win;
     int ep[kPer];
-    classify(xv, i0, n, T, s0, Ab, q, win, ep);
+    classify(xv, i0, n, T, s0, Ab, own, q, win, ep);
     long long qs = 0;
 #pragma unroll
-    for (int k = 0; k < kPer; ++k) qs += q[k];
-    // the binade of the last element's run (the walk's tail check)
-    if (i0 <= n - 1 && n - 1 < i0 + kPer) {
-        const int k = static_cast<int>(n - 1 - i0);
-        *elast = (win >> k) & 1u ? -1 : ep[k];
+    for (int k = 0; k < kPer; ++k) {
+        qs += q[k];
+        // the binade of the last element's run (the walk's tail check)
+        if (i0 + k == n - 1) *elast = (win >> k) & 1u ? -1 : ep[k];
     }
     // descriptor of the event-loop walk: the tile's binade, certain for the
     // whole tile, and its increments at that binade
@@ -173,14 +202,31 @@ __global__ void __launch_bounds__(kDescThreads) k_fold_count(const double *x, ui
     }
     ev = __syncthreads_or(ev);
     A = block_sum(A, shl);
-    qs = block_sum(qs, shl);
-    const unsigned wc = block_sum(static_cast<unsigned>(__popc(win)), shu);
+    long long qtot;
+    unsigned wtot;
+    long long P = block_exclusive_sum(qs, shl, &qtot);
+    unsigned r = block_exclusive_sum(static_cast<unsigned>(__popc(win)), shu, &wtot);
+    if (wtot <= loc.cap) {
+        const uint64_t slot0 = t * loc.cap;
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            if ((win >> k) & 1u) {
+                const uint64_t sl = slot0 + r;
+                loc.off[sl] = threadIdx.x * kPer + k;
+                loc.x[sl] = xv[k];
+                loc.P[sl] = P;
+                loc.e[sl] = ep[k];
+                ++r;
+            }
+            P += q[k];
+        }
+    }
     if (threadIdx.x == 0) {
         desc[t].eb = eb;
         desc[t].flags = (slow || ev) ? 1 : 0;
         desc[t].A = A;
-        tq[t] = qs;
-        tw[t] = wc;
+        tq[t] = qtot;
+        tw[t] = wtot;
     }
 }
 
@@ -217,21 +263,33 @@ __global__ void __launch_bounds__(1024) k_fold_scan_counts(const long long *tq, 
 // 5. the windows in order: index, value, run-increment prefix before it and
 // the binade of the run before it
 __global__ void __launch_bounds__(kDescThreads) k_fold_emit(const double *x, uint64_t n, double s0,
-    const double *tpre, uint64_t T, const long long *pq, const unsigned long long *pw, const long long *tot,
-    FoldWindows w)
+    const double *tpre, uint64_t T, const long long *pq, const unsigned long long *pw, const unsigned *tw,
+    const long long *tot, FoldWindows w, FoldLocal loc)
 {
     __shared__ double shd[33];
     __shared__ long long shl[33];
     __shared__ unsigned shu[33];
     if (static_cast<unsigned long long>(tot[1]) > w.cap) return;  // the walk takes the event loop
     const uint64_t t = blockIdx.x;
+    const unsigned nw = tw[t];
+    if (nw == 0) return;
+    if (nw <= loc.cap) {  // the counting pass listed them
+        for (unsigned k = threadIdx.x; k < nw; k += kDescThreads) {
+            const uint64_t sl = t * loc.cap + k, g = pw[t] + k;
+            w.idx[g] = t * kFoldTile + loc.off[sl];
+            w.x[g] = loc.x[sl];
+            w.P[g] = pq[t] + loc.P[sl];
+            w.e[g] = loc.e[sl];
+        }
+        return;
+    }
     const uint64_t i0 = t * kFoldTile + static_cast<uint64_t>(threadIdx.x) * kPer;
-    double xv[kPer], Ab;
-    tile_load(x, n, s0, tpre, t, xv, shd, &Ab);
+    double xv[kPer], Ab, own;
+    tile_load(x, n, s0, tpre, t, xv, shd, &Ab, &own);
     long long q[kPer];
     unsigned win;
     int ep[kPer];
-    classify(xv, i0, n, T, s0, Ab, q, win, ep);
+    classify(xv, i0, n, T, s0, Ab, own, q, win, ep);
     long long qs = 0;
 #pragma unroll
     for (int k = 0; k < kPer; ++k) qs += q[k];
@@ -563,12 +621,12 @@ __global__ void __launch_bounds__(kDescThreads) k_fold_expand(const double *x, u
         return;
     }
     const uint64_t i0 = t * kFoldTile + static_cast<uint64_t>(threadIdx.x) * kPer;
-    double xv[kPer], Ab;
-    tile_load(x, n, s0, tpre, t, xv, shd, &Ab);
+    double xv[kPer], Ab, own;
+    tile_load(x, n, s0, tpre, t, xv, shd, &Ab, &own);
     long long q[kPer];
     unsigned win;
     int ep[kPer];
-    classify(xv, i0, n, T, s0, Ab, q, win, ep);
+    classify(xv, i0, n, T, s0, Ab, own, q, win, ep);
     long long qs = 0;
 #pragma unroll
     for (int k = 0; k < kPer; ++k) qs += q[k];
@@ -607,16 +665,19 @@ uint64_t fold_window_cap(uint64_t n)
 size_t fold_scratch_bytes(uint64_t n, uint64_t wcap)
 {
     const uint64_t T = (n + kFoldTile - 1) / kFoldTile + 1;
+    const uint64_t L = wcap == 0 ? T * kFoldLocalCap : 0;
     if (wcap == 0) wcap = fold_window_cap(n);
     return align256(T * sizeof(FoldDesc)) + 3 * align256(T * sizeof(double)) + align256(T * sizeof(int)) +
            align256(T * sizeof(long long)) + align256(T * sizeof(unsigned)) + align256(T * sizeof(long long)) +
            align256(T * sizeof(unsigned long long)) + 256 + align256(wcap * sizeof(unsigned long long)) +
-           3 * align256(wcap * sizeof(double)) + align256(wcap * sizeof(int));
+           3 * align256(wcap * sizeof(double)) + align256(wcap * sizeof(int)) + 2 * align256(L * sizeof(int)) +
+           2 * align256(L * sizeof(double));
 }
 
 FoldScratch fold_scratch_carve(void *base, uint64_t n, uint64_t wcap)
 {
     const uint64_t T = (n + kFoldTile - 1) / kFoldTile + 1;
+    const unsigned lcap = wcap == 0 ? kFoldLocalCap : 0;
     if (wcap == 0) wcap = fold_window_cap(n);
     char *p = static_cast<char *>(base);
     auto take = [&p](size_t bytes) {
@@ -645,6 +706,12 @@ FoldScratch fold_scratch_carve(void *base, uint64_t n, uint64_t wcap)
     f.win.S = reinterpret_cast<double *>(take(wcap * sizeof(double)));
     f.win.e = reinterpret_cast<int *>(take(wcap * sizeof(int)));
     f.win.cap = wcap;
+    const uint64_t L = T * lcap;
+    f.loc.off = reinterpret_cast<unsigned *>(take(L * sizeof(unsigned)));
+    f.loc.x = reinterpret_cast<double *>(take(L * sizeof(double)));
+    f.loc.P = reinterpret_cast<long long *>(take(L * sizeof(long long)));
+    f.loc.e = reinterpret_cast<int *>(take(L * sizeof(int)));
+    f.loc.cap = lcap;
     return f;
 }
 
@@ -661,11 +728,12 @@ int fold_exact(const double *x, uint64_t n, double s0, double *prefix, FoldScrat
     MB_LAUNCH_CHECK();
     k_fold_scan_tiles<<<1, 1024, 0, s>>>(fs.tsum, T, fs.tpre);
     MB_LAUNCH_CHECK();
-    k_fold_count<<<nt, kDescThreads, 0, s>>>(x, n, s0, fs.tsum, fs.tpre, T, fs.tq, fs.tw, fs.desc, fs.elast);
+    k_fold_count<<<nt, kDescThreads, 0, s>>>(x, n, s0, fs.tsum, fs.tpre, T, fs.tq, fs.tw, fs.desc, fs.elast,
+        fs.loc);
     MB_LAUNCH_CHECK();
     k_fold_scan_counts<<<1, 1024, 0, s>>>(fs.tq, fs.tw, T, fs.pq, fs.pw, fs.tot);
     MB_LAUNCH_CHECK();
-    k_fold_emit<<<nt, kDescThreads, 0, s>>>(x, n, s0, fs.tpre, T, fs.pq, fs.pw, fs.tot, fs.win);
+    k_fold_emit<<<nt, kDescThreads, 0, s>>>(x, n, s0, fs.tpre, T, fs.pq, fs.pw, fs.tw, fs.tot, fs.win, fs.loc);
     MB_LAUNCH_CHECK();
     k_fold_walk<<<1, kWalkThreads, 0, s>>>(x, n, s0, fs.desc, T, fs.tstart, fs.tmode, prefix, fs.final_v, fs.tot,
         fs.elast, fs.win, fs.mode);

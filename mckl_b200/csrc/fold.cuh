@@ -47,6 +47,7 @@
 namespace mckl_b200 {
 
 constexpr int kFoldTile = 4096;
+constexpr unsigned kFoldLocalCap = 32;
 
 struct FoldDesc {
     int eb;         // biased exponent of the tile's binade (0: subnormal range)
@@ -132,6 +133,19 @@ struct FoldWindows {
     uint64_t cap;
 };
 
+// Per-tile window lists written by the counting pass (capacity `cap` per
+// tile, 0: none): the window's offset in its tile, value, the run-increment
+// sum before it within the tile, and the binade of the run before it.  A tile
+// with at most `cap` windows is placed by copying its list; a fuller one is
+// classified again.
+struct FoldLocal {
+    unsigned *off;
+    double *x;
+    long long *P;
+    int *e;
+    unsigned cap;
+};
+
 struct FoldScratch {
     double *tsum;     // [T] approximate tile sums
     double *tpre;     // [T] approximate exclusive prefix of tile sums
@@ -147,13 +161,16 @@ struct FoldScratch {
     int *mode;        // 0 window walk, 1 event-loop walk
     double *final_v;  // [1] the fold's last value
     FoldWindows win;
+    FoldLocal loc;
 };
 
 // Host driver (fold.cu): folds x[0..n) starting from s0.  `prefix` (device,
 // nullable) receives every partial sum; the last one is also left in
 // scratch.final_v.  Returns an MCKL_B200_* status.  `wcap`: capacity of the
 // window list (0: fold_window_cap(n)); a fold with more windows than that
-// takes the event-loop walk.
+// takes the event-loop walk.  The default sizing (wcap 0) also holds per-tile
+// window lists of kFoldLocalCap entries; an explicit wcap sizes the scratch
+// without them (the tiles with windows are then classified twice).
 int fold_exact(const double *x, uint64_t n, double s0, double *prefix, FoldScratch &fs, cudaStream_t s);
 uint64_t fold_window_cap(uint64_t n);
 size_t fold_scratch_bytes(uint64_t n, uint64_t wcap = 0);

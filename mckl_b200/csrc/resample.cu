@@ -99,9 +99,39 @@ __global__ void k_systematic(G g, Ctr B, uint32_t off, uint64_t M, double *u)
     GRID_LOOP(j, M) { u[j] = __fma_rn(static_cast<double>(j), delta, ud); }
 }
 
-__device__ __forceinline__ uint64_t lower_bound(const double *u, uint64_t M, double v)
+// The first k with u[k] >= v in the sorted u[0..M), found by galloping out
+// from the guess g (any g in [0, M] gives the same answer) and a binary search
+// of the bracket: about 2 log2(|answer - g| + 1) reads.  The uniforms of every
+// scheme are sorted and close to evenly spread over [0, 1) -- within one slot
+// of j/M for the stratified and systematic sequences -- so g = floor(v M) is
+// usually within a step or two, and the reads of a warp are coalesced.
+__device__ __forceinline__ uint64_t lower_bound_from(const double *u, uint64_t M, double v, uint64_t g)
 {
-    uint64_t lo = 0, hi = M;
+    uint64_t lo, hi;
+    if (g < M && u[g] < v) {  // the answer is in (g, M]
+        lo = g + 1;
+        hi = M;
+        for (uint64_t step = 1;; step <<= 1) {
+            const uint64_t probe = lo - 1 + step;
+            if (probe >= M) break;
+            if (u[probe] >= v) {
+                hi = probe;
+                break;
+            }
+            lo = probe + 1;
+        }
+    } else {  // the answer is in [0, g]
+        lo = 0;
+        hi = g;
+        for (uint64_t step = 1; step <= hi; step <<= 1) {
+            const uint64_t probe = hi - step;
+            if (u[probe] < v) {
+                lo = probe + 1;
+                break;
+            }
+            hi = probe;
+        }
+    }
     while (lo < hi) {
         const uint64_t mid = (lo + hi) >> 1;
         if (u[mid] < v) {
@@ -111,6 +141,13 @@ __device__ __forceinline__ uint64_t lower_bound(const double *u, uint64_t M, dou
         }
     }
     return lo;
+}
+
+__device__ __forceinline__ uint64_t lower_bound(const double *u, uint64_t M, double v)
+{
+    const double gx = v * static_cast<double>(M);
+    const uint64_t g = gx > 0.0 ? (gx < static_cast<double>(M) ? static_cast<uint64_t>(gx) : M) : 0;
+    return lower_bound_from(u, M, v, g);
 }
 
 // the neighbouring doubles of v >= 0 (v below the largest finite double)
@@ -133,14 +170,22 @@ __global__ void k_rep_counts(uint64_t N, uint64_t M, const double *c, const doub
 {
     __shared__ unsigned long long sh[33];
     unsigned long long nt = 0;
-    GRID_LOOP(i, N)
-    {
-        const uint64_t prev = i == 0 ? 0 : lower_bound(u, M, c[i - 1]);
-        const uint64_t cur = (i + 1 == N) ? M : lower_bound(u, M, c[i]);
-        rep[i] = cur - prev;
-        if (ties && i + 1 < N) {
-            const double ci = c[i];
-            nt += lower_bound(u, M, next_up(next_up(ci))) - lower_bound(u, M, next_down(ci));
+    // the bound below c[i - 1] is the previous lane's bound below c[i]: one
+    // search per particle, and one more per warp (the loop bound is the same
+    // for the whole CTA, so every lane takes part in the shuffle)
+    for (uint64_t b = static_cast<uint64_t>(blockIdx.x) * blockDim.x; b < N;
+         b += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t i = b + threadIdx.x;
+        uint64_t cur = 0;
+        if (i < N) cur = (i + 1 == N) ? M : lower_bound(u, M, c[i]);
+        uint64_t prev = __shfl_up_sync(0xffffffffu, cur, 1);
+        if (i < N) {
+            if ((threadIdx.x & 31) == 0) prev = i == 0 ? 0 : lower_bound(u, M, c[i - 1]);
+            rep[i] = cur - prev;
+            if (ties && i + 1 < N) {
+                const double ci = c[i];
+                nt += lower_bound_from(u, M, next_up(next_up(ci)), cur) - lower_bound_from(u, M, next_down(ci), cur);
+            }
         }
     }
     if (ties) {
@@ -190,7 +235,7 @@ constexpr int kScanThreads = 256;
 constexpr int kScanPer = 8;
 constexpr int kScanTile = kScanThreads * kScanPer;
 constexpr unsigned long long kFlagAgg = 1ull << 62, kFlagInc = 2ull << 62, kValMask = (1ull << 62) - 1;
-constexpr long long kSpinLimit = 1ll << 26;
+constexpr long long kSpinLimit = 1ll << 22;  // look-back rounds (each a CTA barrier)
 
 // pair of 31-bit counters packed into 62 bits: low = empties, high = surplus
 __device__ __forceinline__ unsigned long long pack(unsigned long long e, unsigned long long s)
@@ -198,72 +243,117 @@ __device__ __forceinline__ unsigned long long pack(unsigned long long e, unsigne
     return e | (s << 31);
 }
 
+// shared-memory index of element o of a scan tile: one pad word per 16
+// elements, so the blocked reads (thread t, elements 8t..8t+7) hit distinct
+// bank pairs except for a 2-way overlap
+__device__ __forceinline__ unsigned scan_pad(unsigned o)
+{
+    return o + (o >> 4);
+}
+
+// Per tile of kScanTile counts: the exclusive prefixes of (empty slot, surplus)
+// pairs, and every G-th surplus prefix into `coarse`.  Loads and stores are coalesced through shared memory; each thread
+// scans kScanPer consecutive elements.  The tile's offset comes from a
+// decoupled look-back done by the whole CTA: its threads read the statuses of
+// kScanThreads predecessors at once, wait while any is unpublished, and add
+// the aggregates back to the nearest inclusive prefix (tiles before tile 0
+// read as an inclusive 0), so with every tile in flight at once a look-back
+// takes tiles / kScanThreads rounds.  Tiles are numbered in the order the
+// CTAs start (an atomic counter), so every predecessor is running or done.
+// The wait is bounded: past kSpinLimit rounds the error word is set and the
+// result is invalid (the host reports it).
 __global__ void __launch_bounds__(kScanThreads) k_rep_scan(uint64_t N, uint64_t K, const uint64_t *rep,
-    uint32_t *ex_empty, uint32_t *ex_surplus, unsigned long long *status, unsigned *tile_counter, int *err)
+    uint32_t *ex_empty, uint32_t *ex_surplus, unsigned long long *status, unsigned *tile_counter, int *err,
+    uint64_t G, uint32_t *coarse)
 {
     __shared__ unsigned long long sh[33];
+    __shared__ unsigned shu[33];
+    __shared__ unsigned long long sv[kScanTile + kScanTile / 16];
     __shared__ unsigned long long sh_excl;
     __shared__ unsigned sh_tile;
     if (threadIdx.x == 0) sh_tile = atomicAdd(tile_counter, 1u);
     __syncthreads();
     const uint64_t tile = sh_tile;
-    const uint64_t base = tile * kScanTile + static_cast<uint64_t>(threadIdx.x) * kScanPer;
-    unsigned long long v[kScanPer];
-    unsigned long long own = 0;
+    const uint64_t base = tile * kScanTile;
 #pragma unroll
     for (int k = 0; k < kScanPer; ++k) {
-        const uint64_t i = base + k;
-        unsigned long long e = 0, s = 0;
+        const unsigned o = k * kScanThreads + threadIdx.x;
+        const uint64_t i = base + o;
+        unsigned long long e = 0, sp = 0;
         if (i < N) {
             const uint64_t r = rep[i];
             if (i < K) {
                 e = (r == 0);
-                s = r > 0 ? r - 1 : 0;
+                sp = r > 0 ? r - 1 : 0;
             } else {
-                s = r;
+                sp = r;
             }
         }
-        v[k] = pack(e, s);
+        sv[scan_pad(o)] = pack(e, sp);
+    }
+    __syncthreads();
+    unsigned long long v[kScanPer];
+    unsigned long long own = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        v[k] = sv[scan_pad(threadIdx.x * kScanPer + k)];
         own += v[k];
     }
     unsigned long long agg;
     const unsigned long long incl = block_inclusive_sum(own, sh, &agg);
-    if (threadIdx.x == 0) {
-        unsigned long long excl = 0;
-        if (tile == 0) {
+    if (tile == 0) {
+        if (threadIdx.x == 0) {
             atomicExch(&status[0], kFlagInc | agg);
-        } else {
-            atomicExch(&status[tile], kFlagAgg | agg);
-            long long p = static_cast<long long>(tile) - 1;
-            long long spins = 0;
-            while (p >= 0) {
-                const unsigned long long st = *reinterpret_cast<volatile unsigned long long *>(&status[p]);
-                const unsigned long long fl = st & ~kValMask;
-                if (fl == 0) {
-                    if (++spins > kSpinLimit) {
-                        atomicExch(err, 1);  // give up: the result is invalid, the host reports it
-                        break;
-                    }
-                    continue;
-                }
-                excl += st & kValMask;
-                if (fl == kFlagInc) break;
-                --p;
-            }
-            atomicExch(&status[tile], kFlagInc | (excl + agg));
+            sh_excl = 0;
         }
-        sh_excl = excl;
+    } else {
+        if (threadIdx.x == 0) atomicExch(&status[tile], kFlagAgg | agg);
+        long long p = static_cast<long long>(tile) - 1;
+        long long spins = 0;
+        bool failed = false;
+        unsigned long long excl = 0;
+        for (;;) {
+            const long long q = p - static_cast<long long>(threadIdx.x);
+            unsigned long long st = 2ull << 62;  // kFlagInc, value 0
+            if (q >= 0) st = *reinterpret_cast<volatile unsigned long long *>(&status[q]);
+            const unsigned long long fl = st & ~kValMask;
+            if (__syncthreads_or(fl == 0)) {
+                if (++spins > kSpinLimit) {
+                    failed = true;
+                    break;
+                }
+                continue;
+            }
+            const unsigned first = block_min_u32(fl == kFlagInc ? threadIdx.x : 0xffffffffu, shu);
+            excl += block_sum(threadIdx.x <= first ? (st & kValMask) : 0ull, sh);
+            if (first != 0xffffffffu) break;
+            p -= kScanThreads;
+        }
+        if (threadIdx.x == 0) {
+            if (failed) atomicExch(err, 1);
+            atomicExch(&status[tile], kFlagInc | (excl + agg));
+            sh_excl = excl;
+        }
     }
     __syncthreads();
     unsigned long long run = sh_excl + incl - own;
 #pragma unroll
     for (int k = 0; k < kScanPer; ++k) {
-        const uint64_t i = base + k;
-        if (i < N) {
-            ex_empty[i] = static_cast<uint32_t>(run & 0x7fffffffull);
-            ex_surplus[i] = static_cast<uint32_t>((run >> 31) & 0x7fffffffull);
-        }
+        sv[scan_pad(threadIdx.x * kScanPer + k)] = run;
         run += v[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        const unsigned o = k * kScanThreads + threadIdx.x;
+        const uint64_t i = base + o;
+        if (i < N) {
+            const unsigned long long x = sv[scan_pad(o)];
+            const uint32_t sp = static_cast<uint32_t>((x >> 31) & 0x7fffffffull);
+            ex_empty[i] = static_cast<uint32_t>(x & 0x7fffffffull);
+            ex_surplus[i] = sp;
+            if (i % G == 0) coarse[i / G] = sp;
+        }
     }
 }
 
@@ -287,44 +377,111 @@ __global__ void k_rep_place(uint64_t N, uint64_t M, uint64_t K, const uint64_t *
     }
 }
 
-// the k-th empty slot takes the source whose surplus range holds k
-__global__ void k_rep_fill(uint64_t N, uint64_t M, uint64_t K, const uint64_t *rep, const uint32_t *ex_empty,
-    const uint32_t *ex_surplus, const uint32_t *empty_pos, uint64_t *idx)
+// The k-th empty slot takes the source whose surplus range holds k: the last
+// s with ex_surplus[s] <= k.  One wave of CTAs, each taking 256 consecutive
+// empties per round.  A CTA first loads the coarse table of the prefixes,
+// coarse[j] = ex_surplus[j G] (at most kCoarse entries, written by the scan),
+// and finds in it the cells holding the sources of its first and last empty;
+// those bound the sources of all of its empties (ex_surplus is
+// nondecreasing).  A bracket of at most kFillStage sources is staged with
+// coalesced loads and every lane searches it in shared memory; a wider one is
+// searched in global memory, still only between the bounds.
+constexpr int kFillThreads = 256, kFillStage = 4096, kCoarse = 2048;
+
+uint64_t coarse_step(uint64_t N)
 {
-    const uint64_t n_empty = (K == 0 ? 0 : ex_empty[K - 1] + (rep[K - 1] == 0 ? 1 : 0)) + (M - K);
-    GRID_LOOP(k, n_empty)
-    {
-        uint64_t lo = 0, hi = N;  // last s with ex_surplus[s] <= k
-        while (hi - lo > 1) {
-            const uint64_t mid = (lo + hi) >> 1;
-            if (ex_surplus[mid] <= k) {
-                lo = mid;
-            } else {
-                hi = mid;
-            }
+    return std::max<uint64_t>(1, (N + kCoarse - 1) / kCoarse);
+}
+
+__device__ __forceinline__ uint64_t surplus_owner(const uint32_t *ex_surplus, uint64_t lo, uint64_t hi, uint64_t k)
+{
+    // ex_surplus[lo] <= k and (hi == N or ex_surplus[hi] > k)
+    while (hi - lo > 1) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if (ex_surplus[mid] <= k) {
+            lo = mid;
+        } else {
+            hi = mid;
         }
-        idx[empty_pos[k]] = lo;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kFillThreads) k_rep_fill(uint64_t N, uint64_t M, uint64_t K, const uint64_t *rep,
+    const uint32_t *ex_empty, const uint32_t *ex_surplus, const uint32_t *empty_pos, uint64_t G,
+    const uint32_t *coarse, uint64_t *idx)
+{
+    __shared__ uint32_t sx[kFillStage];
+    __shared__ uint32_t sc[kCoarse];
+    __shared__ unsigned sh_b[2];
+    const uint64_t n_empty = (K == 0 ? 0 : ex_empty[K - 1] + (rep[K - 1] == 0 ? 1 : 0)) + (M - K);
+    if (static_cast<uint64_t>(blockIdx.x) * kFillThreads >= n_empty) return;
+    const unsigned C = static_cast<unsigned>((N + G - 1) / G);
+    for (unsigned j = threadIdx.x; j < C; j += kFillThreads) sc[j] = coarse[j];
+    __syncthreads();
+    for (uint64_t k0 = static_cast<uint64_t>(blockIdx.x) * kFillThreads; k0 < n_empty;
+         k0 += static_cast<uint64_t>(gridDim.x) * kFillThreads) {
+        const uint64_t klast = std::min<uint64_t>(n_empty, k0 + kFillThreads) - 1;
+        const uint64_t k = k0 + threadIdx.x;
+        const uint32_t dst = k <= klast ? empty_pos[k] : 0;  // issued before the searches
+        if (threadIdx.x < 2) {
+            const uint64_t kk = threadIdx.x == 0 ? k0 : klast;
+            unsigned lo = 0, hi = C;  // sc[0] = 0 <= kk
+            while (hi - lo > 1) {
+                const unsigned mid = (lo + hi) >> 1;
+                if (sc[mid] <= kk) {
+                    lo = mid;
+                } else {
+                    hi = mid;
+                }
+            }
+            sh_b[threadIdx.x] = lo;
+        }
+        __syncthreads();
+        const uint64_t slo = sh_b[0] * G, shi = std::min<uint64_t>(N, (sh_b[1] + 1ull) * G);
+        const uint64_t len = shi - slo;
+        if (len <= kFillStage) {
+            for (uint64_t j = threadIdx.x; j < len; j += kFillThreads) sx[j] = ex_surplus[slo + j];
+            __syncthreads();
+            if (k <= klast) {
+                unsigned lo = 0, hi = static_cast<unsigned>(len);
+                while (hi - lo > 1) {
+                    const unsigned mid = (lo + hi) >> 1;
+                    if (sx[mid] <= k) {
+                        lo = mid;
+                    } else {
+                        hi = mid;
+                    }
+                }
+                idx[dst] = slo + lo;
+            }
+        } else if (k <= klast) {
+            idx[dst] = surplus_owner(ex_surplus, slo, shi, k);
+        }
+        __syncthreads();  // sx and sh_b are rewritten by the next round
     }
 }
 
+// idx[i] == i for every occupied slot, and a copy reads only occupied slots,
+// so no slot is read after it is written
 template <typename T>
 __global__ void k_select_inplace(uint64_t N, uint64_t dim, const uint64_t *idx, T *state)
 {
-    GRID_LOOP(t, N * dim)
+    GRID_LOOP(i, N)
     {
-        const uint64_t d = t / N, i = t % N;
         const uint64_t src = idx[i];
-        if (src != i) state[d * N + i] = state[d * N + src];
+        if (src != i)
+            for (uint64_t d = 0; d < dim; ++d) state[d * N + i] = state[d * N + src];
     }
 }
 
 template <typename T>
 __global__ void k_select_copy(uint64_t N, uint64_t M, uint64_t dim, const uint64_t *idx, const T *in, T *out)
 {
-    GRID_LOOP(t, M * dim)
+    GRID_LOOP(i, M)
     {
-        const uint64_t d = t / M, i = t % M;
-        out[d * M + i] = in[d * N + idx[i]];
+        const uint64_t src = idx[i];
+        for (uint64_t d = 0; d < dim; ++d) out[d * M + i] = in[d * N + src];
     }
 }
 
@@ -487,7 +644,7 @@ size_t rep_index_scratch_bytes(uint64_t N, uint64_t M)
 {
     const uint64_t tiles = (N + kScanTile - 1) / kScanTile + 1;
     return 256 + align256(tiles * sizeof(unsigned long long)) + 2 * align256(N * sizeof(uint32_t)) +
-           align256(M * sizeof(uint32_t)) + 256;
+           align256(M * sizeof(uint32_t)) + align256(kCoarse * sizeof(uint32_t)) + 256;
 }
 
 int rep_to_index_dev(uint64_t N, uint64_t M, const uint64_t *rep, uint64_t *idx, void *scratch_base, int *err_dev,
@@ -506,13 +663,17 @@ int rep_to_index_dev(uint64_t N, uint64_t M, const uint64_t *rep, uint64_t *idx,
     uint32_t *ex_surplus = reinterpret_cast<uint32_t *>(p);
     p += align256(N * sizeof(uint32_t));
     uint32_t *empty_pos = reinterpret_cast<uint32_t *>(p);
+    p += align256(M * sizeof(uint32_t));
+    uint32_t *coarse = reinterpret_cast<uint32_t *>(p);
+    const uint64_t G = coarse_step(N);
     MB_CUDA(cudaMemsetAsync(scratch_base, 0, 256 + align256((tiles + 1) * sizeof(unsigned long long)), s));
     k_rep_scan<<<static_cast<unsigned>(tiles), kScanThreads, 0, s>>>(N, K, rep, ex_empty, ex_surplus, status,
-        tile_counter, err_dev);
+        tile_counter, err_dev, G, coarse);
     MB_LAUNCH_CHECK();
     k_rep_place<<<cap_grid(M, 256), 256, 0, s>>>(N, M, K, rep, ex_empty, idx, empty_pos);
     MB_LAUNCH_CHECK();
-    k_rep_fill<<<cap_grid(M, 256), 256, 0, s>>>(N, M, K, rep, ex_empty, ex_surplus, empty_pos, idx);
+    k_rep_fill<<<cap_grid(M, kFillThreads, 8), kFillThreads, 0, s>>>(N, M, K, rep, ex_empty, ex_surplus, empty_pos,
+        G, coarse, idx);
     MB_LAUNCH_CHECK();
     return MCKL_B200_OK;
 }
@@ -521,9 +682,9 @@ template <typename T>
 int select_dev(uint64_t N, uint64_t M, uint64_t dim, const uint64_t *idx, const T *in, T *out, cudaStream_t s)
 {
     if (N == M && in == out) {
-        k_select_inplace<T><<<cap_grid(N * dim, 256), 256, 0, s>>>(N, dim, idx, out);
+        k_select_inplace<T><<<cap_grid(N, 256), 256, 0, s>>>(N, dim, idx, out);
     } else {
-        k_select_copy<T><<<cap_grid(M * dim, 256), 256, 0, s>>>(N, M, dim, idx, in, out);
+        k_select_copy<T><<<cap_grid(M, 256), 256, 0, s>>>(N, M, dim, idx, in, out);
     }
     MB_LAUNCH_CHECK();
     return MCKL_B200_OK;

@@ -83,23 +83,27 @@ __global__ void __launch_bounds__(32 * kDotWarps) k_weight_chunkdot(uint64_t N, 
 // the CTA fills a tile at a time with coalesced loads
 constexpr int kFinishThreads = 256, kFinishTile = 2048;
 
-__global__ void __launch_bounds__(kFinishThreads) k_weight_finish(uint64_t nchunks, const double *dots,
-    const double *accw, const long long *lmax_bits, double *out /* [ess, log_nc, accw, lmax] */)
+__global__ void __launch_bounds__(kFinishThreads) k_weight_dotsum(uint64_t nchunks, const double *dots, double *essw)
 {
     __shared__ double tile[kFinishTile];
-    double essw = 0.0;
+    double acc = 0.0;
     for (uint64_t t0 = 0; t0 < nchunks; t0 += kFinishTile) {
         const unsigned len = static_cast<unsigned>(nchunks - t0 < kFinishTile ? nchunks - t0 : kFinishTile);
         for (unsigned i = threadIdx.x; i < len; i += kFinishThreads) tile[i] = dots[t0 + i];
         __syncthreads();
         if (threadIdx.x == 0)
-            for (unsigned i = 0; i < len; ++i) essw = __dadd_rn(essw, tile[i]);
+            for (unsigned i = 0; i < len; ++i) acc = __dadd_rn(acc, tile[i]);
         __syncthreads();
     }
-    if (threadIdx.x != 0) return;
+    if (threadIdx.x == 0) *essw = acc;
+}
+
+__global__ void k_weight_finish(const double *essw, const double *accw, const long long *lmax_bits,
+    double *out /* [ess, log_nc, accw, lmax] */)
+{
     const double a = *accw;
     const double lmax = from_ordered_bits(*lmax_bits);
-    out[0] = __ddiv_rn(__dmul_rn(a, a), essw);
+    out[0] = __ddiv_rn(__dmul_rn(a, a), *essw);
     out[1] = __dadd_rn(lmax, dd::log(a));
     out[2] = a;
     out[3] = lmax;
@@ -134,10 +138,11 @@ size_t weight_scratch_bytes(uint64_t N, uint64_t wcap)
 }
 
 int weight_normalize_dev(uint64_t N, double *W, const double *v, int add_log, void *scratch_base,
-    double *result_dev, cudaStream_t s, uint64_t wcap)
+    double *result_dev, cudaStream_t s, uint64_t wcap, const WeightFork *fork)
 {
     char *p = static_cast<char *>(scratch_base);
     long long *lmax_bits = reinterpret_cast<long long *>(p);
+    double *essw = reinterpret_cast<double *>(p + 64);
     const uint64_t nchunks = (N + kChunk - 1) / kChunk;
     double *dots = reinterpret_cast<double *>(p + 256);
     FoldScratch fs = fold_scratch_carve(p + 256 + align256(nchunks * sizeof(double)), N, wcap);
@@ -149,12 +154,22 @@ int weight_normalize_dev(uint64_t N, double *W, const double *v, int add_log, vo
     MB_LAUNCH_CHECK();
     k_weight_exp<<<grid_cap(N, 256), 256, 0, s>>>(N, W, lmax_bits);
     MB_LAUNCH_CHECK();
-    k_weight_chunkdot<<<static_cast<unsigned>((nchunks + kDotWarps - 1) / kDotWarps), 32 * kDotWarps, 0, s>>>(N, W,
-        dots);
+    cudaStream_t ds = s;  // the stream of the ESS's dot products
+    if (fork) {
+        MB_CUDA(cudaEventRecord(fork->fork, s));
+        MB_CUDA(cudaStreamWaitEvent(fork->side, fork->fork, 0));
+        ds = fork->side;
+    }
+    k_weight_chunkdot<<<static_cast<unsigned>((nchunks + kDotWarps - 1) / kDotWarps), 32 * kDotWarps, 0, ds>>>(N,
+        W, dots);
     MB_LAUNCH_CHECK();
+    k_weight_dotsum<<<1, kFinishThreads, 0, ds>>>(nchunks, dots, essw);
+    MB_LAUNCH_CHECK();
+    if (fork) MB_CUDA(cudaEventRecord(fork->join, fork->side));
     int rc = fold_exact(W, N, 0.0, nullptr, fs, s);
     if (rc != MCKL_B200_OK) return rc;
-    k_weight_finish<<<1, kFinishThreads, 0, s>>>(nchunks, dots, fs.final_v, lmax_bits, result_dev);
+    if (fork) MB_CUDA(cudaStreamWaitEvent(s, fork->join, 0));
+    k_weight_finish<<<1, 1, 0, s>>>(essw, fs.final_v, lmax_bits, result_dev);
     MB_LAUNCH_CHECK();
     k_weight_scale<<<grid_cap(N, 256), 256, 0, s>>>(N, W, fs.final_v);
     MB_LAUNCH_CHECK();
