@@ -100,6 +100,50 @@ struct GraphExec {
     }
 };
 
+// The side stream and events of the weight normaliser's fork (the ESS's dot
+// products beside the normaliser's fold), released with the graphs.
+// The plain loop's side stream: the next step's noise and the next
+// resampling's uniforms are drawn there while the main stream runs the
+// current step.  Events: noise[k] -- the noise in buffer k is ready;
+// used[k] -- the step that read buffer k is done with it; u_ready / u_used --
+// the same for the resampling uniforms.
+struct SideWork {
+    cudaStream_t s = nullptr;
+    cudaEvent_t noise[2] = {nullptr, nullptr}, used[2] = {nullptr, nullptr};
+    cudaEvent_t u_ready = nullptr, u_used = nullptr;
+    int create()
+    {
+        MB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        for (cudaEvent_t *e : {&noise[0], &noise[1], &used[0], &used[1], &u_ready, &u_used})
+            MB_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+        return MCKL_B200_OK;
+    }
+    ~SideWork()
+    {
+        if (s) cudaStreamSynchronize(s);  // nothing of ours may run past the call
+        for (cudaEvent_t e : {noise[0], noise[1], used[0], used[1], u_ready, u_used})
+            if (e) cudaEventDestroy(e);
+        if (s) cudaStreamDestroy(s);
+    }
+};
+
+struct OwnedFork {
+    WeightFork f{nullptr, nullptr, nullptr};
+    int create()
+    {
+        MB_CUDA(cudaStreamCreateWithFlags(&f.side, cudaStreamNonBlocking));
+        MB_CUDA(cudaEventCreateWithFlags(&f.fork, cudaEventDisableTiming));
+        MB_CUDA(cudaEventCreateWithFlags(&f.join, cudaEventDisableTiming));
+        return MCKL_B200_OK;
+    }
+    ~OwnedFork()
+    {
+        if (f.join) cudaEventDestroy(f.join);
+        if (f.fork) cudaEventDestroy(f.fork);
+        if (f.side) cudaStreamDestroy(f.side);
+    }
+};
+
 unsigned grid_of(uint64_t n)
 {
     return static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 148 * 16)));
@@ -139,7 +183,7 @@ extern "C" int mckl_b200_pf_ar1_plain_f64(size_t N, size_t T, const double *y, d
     cudaStream_t s = as_stream(stream);
     // work buffers: eps, ll, rep, idx, result words
     const size_t wsz = weight_scratch_bytes(N), rsz = resample_scratch_bytes(N, N), isz = rep_index_scratch_bytes(N, N);
-    const size_t buf = 4 * align256(N * sizeof(double)) + 512 + align256((T + 1) * sizeof(double));
+    const size_t buf = 5 * align256(N * sizeof(double)) + 512 + align256((T + 1) * sizeof(double));
     char *base = static_cast<char *>(scratch(5, buf + wsz + rsz + isz, s));
     if (!base) {
         set_error("particle filter scratch allocation failed");
@@ -154,6 +198,7 @@ extern "C" int mckl_b200_pf_ar1_plain_f64(size_t N, size_t T, const double *y, d
     unsigned long long *ties = reinterpret_cast<unsigned long long *>(base + 4 * align256(N * 8) + 384);
     int *t_dev = reinterpret_cast<int *>(base + 4 * align256(N * 8) + 448);
     double *y_dev = reinterpret_cast<double *>(base + 4 * align256(N * 8) + 512);
+    double *eps2 = reinterpret_cast<double *>(base + 4 * align256(N * 8) + 512 + align256((T + 1) * sizeof(double)));
     void *wscr = base + buf;
     void *rscr = base + buf + wsz;
     void *iscr = base + buf + wsz + rsz;
@@ -191,18 +236,28 @@ extern "C" int mckl_b200_pf_ar1_plain_f64(size_t N, size_t T, const double *y, d
         ResampleScratch rs = resample_scratch_carve(rscr, N, N);
         MB_CUDA(cudaMemcpyAsync(y_dev, y, (T + 1) * sizeof(double), cudaMemcpyHostToDevice, s));
         MB_CUDA(cudaMemsetAsync(t_dev, 0, sizeof(int), s));
-        GraphExec ga, gb;
-        int rc = capture(&ga.e, [&](cudaStream_t c) {
-            k_step_inc<<<1, 1, 0, c>>>(t_dev);
-            MB_LAUNCH_CHECK();
-            k_ar1_propagate_dev<<<grid_of(N), 256, 0, c>>>(N, x_dev, eps, y_dev, t_dev, phi, sx, lconst, hinv, ll);
-            MB_LAUNCH_CHECK();
-            int r = weight_normalize_dev(N, W_dev, ll, 1, wscr, wres, c);
-            if (r != MCKL_B200_OK) return r;
-            MB_CUDA(cudaMemcpyAsync(g_rb.h, wres, 2 * sizeof(double), cudaMemcpyDeviceToHost, c));
-            return MCKL_B200_OK;
-        });
+        double *epsb[2] = {eps, eps2};  // step t reads epsb[t & 1]
+        SideWork side;
+        OwnedFork fork;
+        GraphExec ga[2], gb;
+        int rc = side.create();
         if (rc != MCKL_B200_OK) return rc;
+        rc = fork.create();
+        if (rc != MCKL_B200_OK) return rc;
+        for (int k = 0; k < 2; ++k) {
+            rc = capture(&ga[k].e, [&](cudaStream_t c) {
+                k_step_inc<<<1, 1, 0, c>>>(t_dev);
+                MB_LAUNCH_CHECK();
+                k_ar1_propagate_dev<<<grid_of(N), 256, 0, c>>>(N, x_dev, epsb[k], y_dev, t_dev, phi, sx, lconst, hinv,
+                    ll);
+                MB_LAUNCH_CHECK();
+                int r = weight_normalize_dev(N, W_dev, ll, 1, wscr, wres, c, 0, &fork.f);
+                if (r != MCKL_B200_OK) return r;
+                MB_CUDA(cudaMemcpyAsync(g_rb.h, wres, 2 * sizeof(double), cudaMemcpyDeviceToHost, c));
+                return MCKL_B200_OK;
+            });
+            if (rc != MCKL_B200_OK) return rc;
+        }
         rc = capture(&gb.e, [&](cudaStream_t c) {
             int r = rep_counts_dev(N, N, W_dev, rs.u, rep, rs, c, ties);
             if (r != MCKL_B200_OK) return r;
@@ -215,21 +270,44 @@ extern "C" int mckl_b200_pf_ar1_plain_f64(size_t N, size_t T, const double *y, d
             return MCKL_B200_OK;
         });
         if (rc != MCKL_B200_OK) return rc;
+        // The side stream draws, in the engines' own order, the noise of step
+        // t + 1 while the main stream runs step t, and the uniforms of the
+        // next resampling as soon as the previous one has used its own (they
+        // depend only on the resampling engine's position, which moves only
+        // at a resampling).  The main stream waits for each before use.
+        auto next_uniforms = [&]() -> int {
+            MB_CUDA(cudaStreamWaitEvent(side.s, side.u_used, 0));
+            const int r = u01_sequence_dev(seq_of[scheme], er, N, rs.u, rs.tmp, rs.fs, side.s);
+            if (r != MCKL_B200_OK) return r;
+            MB_CUDA(cudaEventRecord(side.u_ready, side.s));
+            return MCKL_B200_OK;
+        };
+        // x_0 on the main stream, then the noise of step 1 and the first
+        // uniforms beside it (the model engine's order: x_0, then step 1's draws)
+        rc = mckl_b200_normal_f64(&em, N, x_dev, 0.0, sd0, stream);
+        if (rc != MCKL_B200_OK) return rc;
+        MB_CUDA(cudaEventRecord(side.used[0], s));
+        MB_CUDA(cudaStreamWaitEvent(side.s, side.used[0], 0));
+        if (T > 0) {
+            rc = mckl_b200_normal_f64(&em, N, epsb[1], 0.0, 1.0, side.s);
+            if (rc != MCKL_B200_OK) return rc;
+            MB_CUDA(cudaEventRecord(side.noise[1], side.s));
+        }
+        rc = next_uniforms();
+        if (rc != MCKL_B200_OK) return rc;
         for (size_t it = 0; it <= T; ++it) {
-            if (it == 0) {
-                rc = mckl_b200_normal_f64(&em, N, x_dev, 0.0, sd0, stream);
-                if (rc != MCKL_B200_OK) return rc;
-                if (T > 0) {
-                    rc = mckl_b200_normal_f64(&em, N, eps, 0.0, 1.0, stream);
-                    if (rc != MCKL_B200_OK) return rc;
-                }
-            } else {
-                MB_CUDA(cudaGraphLaunch(ga.e, s));
+            if (it > 0) {
+                const int k = static_cast<int>(it & 1);
+                MB_CUDA(cudaStreamWaitEvent(s, side.noise[k], 0));
+                MB_CUDA(cudaGraphLaunch(ga[k].e, s));
                 count_launch();
+                MB_CUDA(cudaEventRecord(side.used[k], s));
                 MB_CUDA(cudaEventRecord(g_rb.ev, s));
-                if (it < T) {
-                    rc = mckl_b200_normal_f64(&em, N, eps, 0.0, 1.0, stream);
+                if (it < T) {  // step it + 1's noise, into the buffer step it - 1 read
+                    MB_CUDA(cudaStreamWaitEvent(side.s, side.used[k ^ 1], 0));
+                    rc = mckl_b200_normal_f64(&em, N, epsb[k ^ 1], 0.0, 1.0, side.s);
                     if (rc != MCKL_B200_OK) return rc;
+                    MB_CUDA(cudaEventRecord(side.noise[k ^ 1], side.s));
                 }
                 MB_CUDA(cudaEventSynchronize(g_rb.ev));
                 ess = g_rb.h[0];
@@ -238,10 +316,14 @@ extern "C" int mckl_b200_pf_ar1_plain_f64(size_t N, size_t T, const double *y, d
             if (ess_hist) ess_hist[it] = ess;
             if (resampled) resampled[it] = 0;
             if (ess < static_cast<double>(N) * threshold) {
-                rc = u01_sequence_dev(seq_of[scheme], er, N, rs.u, rs.tmp, rs.fs, s);
-                if (rc != MCKL_B200_OK) return rc;
+                MB_CUDA(cudaStreamWaitEvent(s, side.u_ready, 0));
                 MB_CUDA(cudaGraphLaunch(gb.e, s));
                 count_launch();
+                MB_CUDA(cudaEventRecord(side.u_used, s));
+                if (it < T) {
+                    rc = next_uniforms();
+                    if (rc != MCKL_B200_OK) return rc;
+                }
                 if (anc_dev) {
                     MB_CUDA(cudaMemcpyAsync(anc_dev + it * N, idx, N * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
                 }
