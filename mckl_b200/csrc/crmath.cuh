@@ -36,6 +36,14 @@
 #else
 #define MB_HD inline
 #endif
+// The accurate phases behind a quick phase run for a few arguments in a
+// thousand: kept out of line on the device, so that they do not add to the
+// register pressure of the kernels that inline the quick phase.
+#if defined(__CUDACC__)
+#define MB_HD_COLD __host__ __device__ __noinline__
+#else
+#define MB_HD_COLD inline
+#endif
 
 #if defined(__CUDA_ARCH__)
 #define MB_ADD(a, b) __dadd_rn((a), (b))
@@ -223,9 +231,10 @@ MB_HD double scale2(double y, int k)
     return MB_MUL(y, MB_FROM_BITS(static_cast<long long>(k + 1023) << 52));
 }
 
-// Correctly rounded (see header) exponential for normal results; results in
-// the subnormal range are rounded twice.
-MB_HD double exp(double x)
+// The accurate phase of exp: the double-double evaluation below, correctly
+// rounded (see header) for normal results; results in the subnormal range are
+// rounded twice.
+MB_HD_COLD double exp_dd(double x)
 {
     if (x != x) return x;
     if (x > 709.782712893384) return MB_FROM_BITS(0x7ff0000000000000ll);
@@ -259,6 +268,90 @@ MB_HD double exp(double x)
     return scale2(MB_ADD(res.hi, res.lo), k);
 }
 
+// Table of the quick phase: {hi, lo} of 2^(j/64), j = 0..63 (exp_table.inc,
+// written by gen_exp_table.py), in global memory on the device like kLogTab.
+#if defined(__CUDACC__)
+static __device__ const double kExpTab[64][2] = {
+#include "exp_table.inc"
+};
+#endif
+#if !defined(__CUDA_ARCH__)
+static const double kExpTabHost[64][2] = {
+#include "exp_table.inc"
+};
+#endif
+#if defined(__CUDA_ARCH__)
+#define MB_EXPTAB(j, k) __ldg(&kExpTab[(j)][(k)])
+#else
+#define MB_EXPTAB(j, k) kExpTabHost[(j)][(k)]
+#endif
+
+// Ziv's rounding test: v.hi = RN(v.hi + v.lo), and v approximates a value
+// to within 2^-62 relative.  True when every value that close rounds to v.hi,
+// i.e. when v.hi is the correctly rounded value.  Below a power of two the
+// gap to the next double is half as wide, so the test uses a quarter ulp on
+// that side.  Zero and subnormal v.hi fail.
+MB_HD bool ziv_ok(const DD &v)
+{
+    const long long b = MB_AS_BITS(v.hi) & 0x7fffffffffffffffll;  // |v.hi|
+    const double u = MB_MUL(MB_FROM_BITS(b & 0x7ff0000000000000ll), 0x1p-52);  // ulp(v.hi)
+    const bool inward = v.hi > 0.0 ? v.lo < 0.0 : v.lo > 0.0;
+    const double half = ((b & 0x000fffffffffffffll) == 0 && inward) ? MB_MUL(u, 0.25) : MB_MUL(u, 0.5);
+    const double d = v.lo < 0.0 ? -v.lo : v.lo;
+    return MB_ADD(d, MB_MUL(MB_FROM_BITS(b), 0x1p-62)) < half;
+}
+
+constexpr double kExpInvL = 0x1.71547652b82fep+6;  // 64 / ln2
+constexpr double kExpL1 = 0x1.62e42fefa0000p-7;    // ln2/64 to 36 bits: k * kExpL1 exact for |k| < 2^17
+constexpr double kExpL2 = 0x1.cf79abc9e3b3ap-46;   // RN(ln2/64 - kExpL1)
+
+// The quick phase of exp: Tang's table-driven method (P. T. P. Tang, ACM TOMS
+// 15(2), 1989) with Ziv's rounding test (A. Ziv, ACM TOMS 17(3), 1991).
+// x = k ln2/64 + r, k = 64 m + j, |r| <= ln2/128: the reduction is exact to
+// 2^-78 (r_hi = x - k L1 exactly by Sterbenz's lemma, the k L2 term in a
+// two_sum), exp(r) - 1 - r_hi is a degree-6 Taylor polynomial (truncation
+// below 2^-65) plus r_lo, and 2^(j/64) (1 + r_hi + p) is summed with the
+// leading product exact.  The total relative error is below 2^-64.4; the
+// result is taken only when the double nearest to the approximation is the
+// same for every value within 2^-62 relative of it, which makes it the
+// correctly rounded exp(x) -- the value the accurate phase returns there
+// too, as the exact result is then far from any rounding midpoint.  About
+// one argument in 500 fails the test and goes to the accurate phase; so do
+// arguments whose result is not a normal double (outside [-708, 709]).
+MB_HD bool exp_quick(double x, double *y)
+{
+    if (!(x >= -708.0 && x <= 709.0)) return false;
+    const double kd = MB_RINT(MB_MUL(x, kExpInvL));
+    const int k = static_cast<int>(kd);
+    const double rh0 = MB_FMA(-kd, kExpL1, x);  // exact
+    const DD r = two_sum(rh0, MB_MUL(-kd, kExpL2));
+    const double rh = r.hi;
+    double P = 0x1.6c16c16c16c17p-10;         // 1/720
+    P = MB_FMA(P, rh, 0x1.1111111111111p-7);  // 1/120
+    P = MB_FMA(P, rh, 0x1.5555555555555p-5);  // 1/24
+    P = MB_FMA(P, rh, 0x1.5555555555555p-3);  // 1/6
+    P = MB_FMA(P, rh, 0.5);
+    const double p = MB_FMA(MB_MUL(rh, rh), P, r.lo);  // exp(r) - 1 - r_hi
+    const int j = k & 63, m = k >> 6;                   // k = 64 m + j, m = floor(k / 64)
+    const double Th = MB_EXPTAB(j, 0), Tl = MB_EXPTAB(j, 1);
+    const DD a = two_prod(Th, rh);
+    const DD s = two_sum(Th, a.hi);
+    const double t = MB_ADD(s.lo, MB_ADD(a.lo, MB_FMA(Th, p, MB_FMA(Tl, MB_ADD(rh, p), Tl))));
+    const DD v = fast_two_sum(s.hi, t);
+    if (!ziv_ok(v)) return false;
+    *y = MB_MUL(v.hi, MB_FROM_BITS(static_cast<long long>(m + 1023) << 52));  // exact: a normal result
+    return true;
+}
+
+// Correctly rounded (see header) exponential: the quick phase, else the
+// accurate one.
+MB_HD double exp(double x)
+{
+    double y;
+    if (exp_quick(x, &y)) return y;
+    return exp_dd(x);
+}
+
 // ---------------------------------------------------------------------------
 constexpr double kTwoOverPi = 0x1.45f306dc9c883p-1;
 constexpr double kPio2P1 = 0x1.921fb54400000p+0;  // 33 significant bits
@@ -266,9 +359,10 @@ constexpr double kPio2P2 = 0x1.0b4611a600000p-34; // 33 significant bits
 constexpr double kPio2P3 = 0x1.3198a2e037073p-69;
 constexpr double kPio2P4 = 0x1.129024e088a68p-123;
 
-// sin and cos of a double, correctly rounded (see header) for |x| < 1e5;
-// larger arguments fall back to the device library.
-MB_HD void sincos(double x, double *sp, double *cp)
+// The accurate phase of sincos: sin and cos of a double in double-double,
+// correctly rounded (see header) for |x| < 1e5; larger arguments fall back to
+// the device library.
+MB_HD_COLD void sincos_dd(double x, double *sp, double *cp)
 {
     if (!(x < 1e5 && x > -1e5)) {
         MB_LIB_SINCOS(x, sp, cp);
@@ -319,6 +413,104 @@ MB_HD void sincos(double x, double *sp, double *cp)
         case 2: *sp = -s; *cp = -c; break;
         default: *sp = -c; *cp = s; break;
     }
+}
+
+// Table of the quick phase: {sin hi, lo, cos hi, lo} of j/64, j = 0..51
+// (sincos_table.inc, written by gen_sincos_table.py), in global memory on the
+// device like kLogTab.
+#if defined(__CUDACC__)
+static __device__ const double kSinCosTab[52][4] = {
+#include "sincos_table.inc"
+};
+#endif
+#if !defined(__CUDA_ARCH__)
+static const double kSinCosTabHost[52][4] = {
+#include "sincos_table.inc"
+};
+#endif
+#if defined(__CUDA_ARCH__)
+#define MB_SCTAB(j, k) __ldg(&kSinCosTab[(j)][(k)])
+#else
+#define MB_SCTAB(j, k) kSinCosTabHost[(j)][(k)]
+#endif
+
+// The quick phase of sincos: the accurate phase's reduction to r = x - k pi/2
+// (a double-double, |r| <= pi/4), then |r| = j/64 + b with |b| <= 1/128
+// (b_hi = |r_hi| - j/64 exactly, by Sterbenz's lemma for j >= 1) and the
+// angle-addition formulas over the table's sin(j/64), cos(j/64):
+//   sin|r| = S + C b_h + [S_l + C_l b_h + C b_l - S b_h b_l + S (cos b_h - 1) + C (sin b_h - b_h)]
+//   cos|r| = C - S b_h + [C_l - S_l b_h - S b_l - C b_h b_l + C (cos b_h - 1) - S (sin b_h - b_h)]
+// with the leading products exact (two_prod) and cos b_h - 1, sin b_h - b_h
+// Taylor polynomials in b_h^2 (truncation below 2^-70 relative).  The
+// bracketed tails are below 2^-14 of the results, so their roundings stay
+// below 2^-64 relative.  Both values are taken only when Ziv's test passes for
+// both (then each is the correctly rounded value, as the accurate phase's);
+// otherwise the call goes to the accurate phase.
+MB_HD bool sincos_quick(double x, double *sp, double *cp)
+{
+    if (!(x < 1e5 && x > -1e5)) return false;
+    const double kd = MB_RINT(MB_MUL(x, kTwoOverPi));
+    const double t = MB_FMA(-kd, kPio2P1, x);  // exact
+    const DD p2 = two_prod(-kd, kPio2P2);
+    DD r = two_sum(t, p2.hi);
+    r.lo = MB_ADD(r.lo, p2.lo);
+    r.lo = MB_FMA(-kd, kPio2P3, r.lo);
+    r.lo = MB_FMA(-kd, kPio2P4, r.lo);
+    r = fast_two_sum(r.hi, r.lo);
+    const bool neg = r.hi < 0.0;
+    const double ah = neg ? -r.hi : r.hi, bl = neg ? -r.lo : r.lo;  // |r| = ah + bl
+    const double jd = MB_RINT(MB_MUL(ah, 64.0));
+    if (!(jd <= 51.0)) return false;
+    const int j = static_cast<int>(jd);
+    const double bh = MB_SUB(ah, MB_MUL(jd, 0.015625));  // exact
+    const double w = MB_MUL(bh, bh);
+    double Pc = 0x1.a01a01a01a01ap-16;           // 1/40320
+    Pc = MB_FMA(Pc, w, -0x1.6c16c16c16c17p-10);  // -1/720
+    Pc = MB_FMA(Pc, w, 0x1.5555555555555p-5);    // 1/24
+    Pc = MB_FMA(Pc, w, -0.5);
+    double Ps = 0x1.71de3a556c734p-19;           // 1/362880
+    Ps = MB_FMA(Ps, w, -0x1.a01a01a01a01ap-13);  // -1/5040
+    Ps = MB_FMA(Ps, w, 0x1.1111111111111p-7);    // 1/120
+    Ps = MB_FMA(Ps, w, -0x1.5555555555555p-3);   // -1/6
+    const double cm1 = MB_MUL(w, Pc);             // cos b_h - 1
+    const double smb = MB_MUL(bh, MB_MUL(w, Ps));  // sin b_h - b_h
+    const double bbl = MB_MUL(bh, bl);
+    const double Sh = MB_SCTAB(j, 0), Sl = MB_SCTAB(j, 1), Ch = MB_SCTAB(j, 2), Cl = MB_SCTAB(j, 3);
+    const DD p = two_prod(Ch, bh);
+    const DD sa = two_sum(Sh, p.hi);
+    double ts = MB_FMA(Cl, bh, Sl);
+    ts = MB_FMA(-Sh, bbl, ts);
+    ts = MB_FMA(Ch, bl, ts);
+    ts = MB_FMA(Ch, smb, ts);
+    ts = MB_FMA(Sh, cm1, ts);
+    ts = MB_ADD(MB_ADD(sa.lo, p.lo), ts);
+    const DD sv = fast_two_sum(sa.hi, ts);
+    const DD q = two_prod(Sh, bh);
+    const DD ca = two_sum(Ch, -q.hi);
+    double tc = MB_FMA(-Sl, bh, Cl);
+    tc = MB_FMA(-Ch, bbl, tc);
+    tc = MB_FMA(-Sh, bl, tc);
+    tc = MB_FMA(-Sh, smb, tc);
+    tc = MB_FMA(Ch, cm1, tc);
+    tc = MB_ADD(MB_SUB(ca.lo, q.lo), tc);
+    const DD cv = fast_two_sum(ca.hi, tc);
+    if (!ziv_ok(sv) || !ziv_ok(cv)) return false;
+    const double s = neg ? -sv.hi : sv.hi, c = cv.hi;
+    switch (static_cast<int>(static_cast<long long>(kd) & 3)) {
+        case 0: *sp = s; *cp = c; break;
+        case 1: *sp = c; *cp = -s; break;
+        case 2: *sp = -s; *cp = -c; break;
+        default: *sp = -c; *cp = s; break;
+    }
+    return true;
+}
+
+// sin and cos of a double, correctly rounded (see header): the quick phase,
+// else the accurate one.
+MB_HD void sincos(double x, double *sp, double *cp)
+{
+    if (sincos_quick(x, sp, cp)) return;
+    sincos_dd(x, sp, cp);
 }
 
 MB_HD double cos(double x)
