@@ -424,7 +424,10 @@ def bench_plain_c3(N=1 << 20, T=1000):
             "scan_ties_note": "uniforms within one representable step of a cumulative weight, over all resampling "
                               "steps; the cumulative weights are the reference's sequential fold bit for bit, so "
                               "a tie flips no ancestor",
-            "bound": "host round trip per step (the reference's step order: normaliser and ESS read back)",
+            "bound": "latency: per step a chain of ~25 dependent kernels (the exact sequential folds walk their "
+                     "windows on one thread) and one host read-back of (ESS, log normaliser), the reference's step "
+                     "order; the next step's noise and the next resampling's uniforms run beside it on a second "
+                     "stream",
             "y": y}
 
 

@@ -40,7 +40,7 @@
 // thousand: kept out of line on the device, so that they do not add to the
 // register pressure of the kernels that inline the quick phase.
 #if defined(__CUDACC__)
-#define MB_HD_COLD __host__ __device__ __noinline__
+#define MB_HD_COLD inline __host__ __device__ __noinline__
 #else
 #define MB_HD_COLD inline
 #endif
