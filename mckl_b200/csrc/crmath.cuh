@@ -233,8 +233,9 @@ MB_HD double scale2(double y, int k)
 
 // The accurate phase of exp: the double-double evaluation below, correctly
 // rounded (see header) for normal results; results in the subnormal range are
-// rounded twice.
-MB_HD_COLD double exp_dd(double x)
+// rounded twice.  exp_dd_inline is the same evaluation inlined (for kernels
+// that call it on every value and measured faster so).
+MB_HD double exp_dd_inline(double x)
 {
     if (x != x) return x;
     if (x > 709.782712893384) return MB_FROM_BITS(0x7ff0000000000000ll);
@@ -266,6 +267,11 @@ MB_HD_COLD double exp_dd(double x)
     }
     const DD res = add_d(E, 1.0);
     return scale2(MB_ADD(res.hi, res.lo), k);
+}
+
+MB_HD_COLD double exp_dd(double x)
+{
+    return exp_dd_inline(x);
 }
 
 // Table of the quick phase: {hi, lo} of 2^(j/64), j = 0..63 (exp_table.inc,
@@ -361,8 +367,8 @@ constexpr double kPio2P4 = 0x1.129024e088a68p-123;
 
 // The accurate phase of sincos: sin and cos of a double in double-double,
 // correctly rounded (see header) for |x| < 1e5; larger arguments fall back to
-// the device library.
-MB_HD_COLD void sincos_dd(double x, double *sp, double *cp)
+// the device library.  sincos_dd_inline is the same evaluation inlined.
+MB_HD void sincos_dd_inline(double x, double *sp, double *cp)
 {
     if (!(x < 1e5 && x > -1e5)) {
         MB_LIB_SINCOS(x, sp, cp);
@@ -413,6 +419,11 @@ MB_HD_COLD void sincos_dd(double x, double *sp, double *cp)
         case 2: *sp = -s; *cp = -c; break;
         default: *sp = -c; *cp = s; break;
     }
+}
+
+MB_HD_COLD void sincos_dd(double x, double *sp, double *cp)
+{
+    sincos_dd_inline(x, sp, cp);
 }
 
 // Table of the quick phase: {sin hi, lo, cos hi, lo} of j/64, j = 0..51
