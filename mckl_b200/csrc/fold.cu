@@ -75,8 +75,9 @@ __device__ __forceinline__ void tile_load(const double *x, uint64_t n, double s0
 // every element's binade is certain and the same, and only its increment
 // remains to be checked.
 __device__ __forceinline__ void classify(const double (&xv)[kPer], uint64_t i0, uint64_t n, uint64_t T, double s0,
-    double Abefore, double own, long long (&q)[kPer], unsigned &win, int (&eprev)[kPer])
+    double Abefore, double own, long long (&q)[kPer], unsigned &win, int (&eprev)[kPer], int *fast_e = nullptr)
 {
+    if (fast_e) *fast_e = -1;
     {
         const double Aend = __dadd_rn(Abefore, own);
         const double c = 2.0 * static_cast<double>(i0 + kPer) + 2.0 * static_cast<double>(T) + 160.0;
@@ -94,6 +95,7 @@ __device__ __forceinline__ void classify(const double (&xv)[kPer], uint64_t i0, 
                     win |= 1u << k;
                 }
             }
+            if (fast_e) *fast_e = e;
             return;
         }
     }
@@ -171,7 +173,8 @@ __global__ void __launch_bounds__(kDescThreads) k_fold_count(const double *x, ui
     long long q[kPer];
     unsigned win;
     int ep[kPer];
-    classify(xv, i0, n, T, s0, Ab, own, q, win, ep);
+    int fe;
+    classify(xv, i0, n, T, s0, Ab, own, q, win, ep, &fe);
     long long qs = 0;
 #pragma unroll
     for (int k = 0; k < kPer; ++k) {
@@ -188,9 +191,19 @@ __global__ void __launch_bounds__(kDescThreads) k_fold_count(const double *x, ui
     int slow = !(lo > 0.0);
     const int eb = biased_exp(lo);
     if (biased_exp(hi) != eb) slow = 1;
-    long long A = 0;
-    int ev = 0;
-    if (!slow) {
+    long long qtot;
+    unsigned wtot;
+    long long P = block_exclusive_sum(qs, shl, &qtot);
+    unsigned r = block_exclusive_sum(static_cast<unsigned>(__popc(win)), shu, &wtot);
+    // When every thread classified its range in the tile's binade, the
+    // descriptor's increments are the run increments just summed (the
+    // windows are then exactly the elements with an event); otherwise they
+    // are formed at the tile's binade.  `slow` is the same for the whole CTA.
+    long long A = qtot;
+    int ev = wtot > 0;
+    if (!slow && !__syncthreads_and(fe == eb)) {
+        A = 0;
+        ev = 0;
 #pragma unroll
         for (int k = 0; k < kPer; ++k) {
             if (i0 + k < n) {
@@ -199,13 +212,9 @@ __global__ void __launch_bounds__(kDescThreads) k_fold_count(const double *x, ui
                 ev |= e;
             }
         }
+        ev = __syncthreads_or(ev);
+        A = block_sum(A, shl);
     }
-    ev = __syncthreads_or(ev);
-    A = block_sum(A, shl);
-    long long qtot;
-    unsigned wtot;
-    long long P = block_exclusive_sum(qs, shl, &qtot);
-    unsigned r = block_exclusive_sum(static_cast<unsigned>(__popc(win)), shu, &wtot);
     if (wtot <= loc.cap) {
         const uint64_t slot0 = t * loc.cap;
 #pragma unroll
@@ -534,23 +543,44 @@ __global__ void __launch_bounds__(kWalkThreads) k_fold_walk(const double *x, uin
     __shared__ double sh_s;
     __shared__ long long sh_p;
     __shared__ unsigned long long sh_j;
-    const unsigned long long W = static_cast<unsigned long long>(tot[1]);
+    __shared__ unsigned long long sh_w;
+    __shared__ long long sh_q;
+    __shared__ int sh_elast;
+    // The first round's windows are staged before their count is known
+    // (entries past the count are loaded but never read), in the same round
+    // trip as the count and the tail's inputs.
+    {
+        const unsigned m0 = static_cast<unsigned>(w.cap < kStage ? w.cap : kStage);
+        for (unsigned k = threadIdx.x; k < m0; k += blockDim.x) {
+            sj[k] = w.idx[k];
+            sx[k] = w.x[k];
+            sp[k] = w.P[k];
+            se[k] = w.e[k];
+        }
+    }
     if (threadIdx.x == 0) {
-        sh_ok = W <= w.cap ? 1 : 0;
+        const unsigned long long W0 = static_cast<unsigned long long>(tot[1]);
+        sh_w = W0;
+        sh_q = tot[0];
+        sh_elast = *elast;
+        sh_ok = W0 <= w.cap ? 1 : 0;
         sh_s = s0;
         sh_p = 0;
         sh_j = 0;
     }
     __syncthreads();
+    const unsigned long long W = sh_w;
     for (unsigned long long c0 = 0; sh_ok && c0 < W; c0 += kStage) {
         const unsigned m = static_cast<unsigned>(W - c0 < kStage ? W - c0 : kStage);
-        for (unsigned k = threadIdx.x; k < m; k += blockDim.x) {
-            sj[k] = w.idx[c0 + k];
-            sx[k] = w.x[c0 + k];
-            sp[k] = w.P[c0 + k];
-            se[k] = w.e[c0 + k];
+        if (c0 > 0) {
+            for (unsigned k = threadIdx.x; k < m; k += blockDim.x) {
+                sj[k] = w.idx[c0 + k];
+                sx[k] = w.x[c0 + k];
+                sp[k] = w.P[c0 + k];
+                se[k] = w.e[c0 + k];
+            }
+            __syncthreads();
         }
-        __syncthreads();
         if (threadIdx.x == 0) {
             double s = sh_s;
             long long p = sh_p;
@@ -585,8 +615,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_fold_walk(const double *x, uin
     if (threadIdx.x == 0 && sh_ok) {
         double s = sh_s;
         if (sh_j < n) {  // the run after the last window
-            const int e = *elast;
-            const long long K = grid_count(s) + (tot[0] - sh_p);
+            const int e = sh_elast;
+            const long long K = grid_count(s) + (sh_q - sh_p);
             if (e < 0 || !(s > 0.0) || biased_exp(s) != e || K >= grid_top(e)) {
                 sh_ok = 0;
             } else {
