@@ -47,6 +47,36 @@ inline cudaStream_t as_stream(void *s)
     return reinterpret_cast<cudaStream_t>(s);
 }
 
+// ---- programmatic dependent launch -----------------------------------------
+// The SMC step's kernels form long chains of small dependent launches.  A
+// kernel of such a chain is launched with programmatic stream serialisation
+// (launch_pdl), so that its launch and CTA set-up overlap the end of the
+// kernel before it, and begins with pdl_wait(), which returns once that
+// kernel has completed and its writes are visible.  pdl_wait() is a no-op in
+// a kernel launched the ordinary way, so the same kernels serve both.
+__device__ __forceinline__ void pdl_wait()
+{
+#if defined(__CUDA_ARCH__)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+#endif
+}
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args &&...args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = s == nullptr ? 0 : 1;  // the legacy default stream: an ordinary launch
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<Args &&>(args)...);
+}
+
 // ---- engine geometry -------------------------------------------------------
 struct Geom {
     int M;          // result words per block

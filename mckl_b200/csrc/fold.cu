@@ -129,6 +129,7 @@ __device__ __forceinline__ void classify(const double (&xv)[kPer], uint64_t i0, 
 // 1. approximate tile sums
 __global__ void __launch_bounds__(kDescThreads) k_fold_tilesum(const double *x, uint64_t n, double *tsum)
 {
+    pdl_wait();
     __shared__ double sh[33];
     const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kFoldTile;
     double acc = 0;
@@ -143,6 +144,7 @@ __global__ void __launch_bounds__(kDescThreads) k_fold_tilesum(const double *x, 
 // 2. exclusive prefix of the tile sums (one CTA), formed without subtraction
 __global__ void __launch_bounds__(1024) k_fold_scan_tiles(const double *tsum, uint64_t T, double *tpre)
 {
+    pdl_wait();
     __shared__ double sh[33];
     double carry = 0;
     for (uint64_t b = 0; b < T; b += blockDim.x) {
@@ -162,6 +164,7 @@ __global__ void __launch_bounds__(kDescThreads) k_fold_count(const double *x, ui
     const double *tsum, const double *tpre, uint64_t T, long long *tq, unsigned *tw, FoldDesc *desc, int *elast,
     FoldLocal loc)
 {
+    pdl_wait();
     __shared__ double shd[33];
     __shared__ long long shl[33];
     __shared__ unsigned shu[33];
@@ -244,6 +247,7 @@ __global__ void __launch_bounds__(kDescThreads) k_fold_count(const double *x, ui
 __global__ void __launch_bounds__(1024) k_fold_scan_counts(const long long *tq, const unsigned *tw, uint64_t T,
     long long *pq, unsigned long long *pw, long long *tot)
 {
+    pdl_wait();
     __shared__ long long shl[33];
     __shared__ unsigned long long shu[33];
     long long cq = 0;
@@ -275,6 +279,7 @@ __global__ void __launch_bounds__(kDescThreads) k_fold_emit(const double *x, uin
     const double *tpre, uint64_t T, const long long *pq, const unsigned long long *pw, const unsigned *tw,
     const long long *tot, FoldWindows w, FoldLocal loc)
 {
+    pdl_wait();
     __shared__ double shd[33];
     __shared__ long long shl[33];
     __shared__ unsigned shu[33];
@@ -535,6 +540,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_fold_walk(const double *x, uin
     const FoldDesc *desc, uint64_t T, double *tstart, int *tmode, double *prefix, double *final_v,
     const long long *tot, const int *elast, FoldWindows w, int *mode)
 {
+    pdl_wait();
     __shared__ unsigned long long sj[kStage];
     __shared__ double sx[kStage];
     __shared__ long long sp[kStage];
@@ -642,6 +648,7 @@ __global__ void __launch_bounds__(kDescThreads) k_fold_expand(const double *x, u
     const double *tpre, uint64_t T, const long long *pq, const unsigned long long *pw, FoldWindows w,
     const int *mode, const FoldDesc *desc, const double *tstart, const int *tmode, double *prefix)
 {
+    pdl_wait();
     __shared__ double shd[33];
     __shared__ long long shl[33];
     __shared__ unsigned shu[33];
@@ -682,6 +689,7 @@ __global__ void __launch_bounds__(kDescThreads) k_fold_expand(const double *x, u
 
 __global__ void k_fold_set(double *v, double s0)
 {
+    pdl_wait();
     *v = s0;
 }
 
@@ -748,29 +756,29 @@ FoldScratch fold_scratch_carve(void *base, uint64_t n, uint64_t wcap)
 int fold_exact(const double *x, uint64_t n, double s0, double *prefix, FoldScratch &fs, cudaStream_t s)
 {
     if (n == 0) {
-        k_fold_set<<<1, 1, 0, s>>>(fs.final_v, s0);
+        MB_CUDA(launch_pdl(k_fold_set, 1, 1, 0, s, fs.final_v, s0));
         MB_LAUNCH_CHECK();
         return MCKL_B200_OK;
     }
     const uint64_t T = (n + kFoldTile - 1) / kFoldTile;
     const unsigned nt = static_cast<unsigned>(T);
-    k_fold_tilesum<<<nt, kDescThreads, 0, s>>>(x, n, fs.tsum);
+    MB_CUDA(launch_pdl(k_fold_tilesum, nt, kDescThreads, 0, s, x, n, fs.tsum));
     MB_LAUNCH_CHECK();
-    k_fold_scan_tiles<<<1, 1024, 0, s>>>(fs.tsum, T, fs.tpre);
+    MB_CUDA(launch_pdl(k_fold_scan_tiles, 1, 1024, 0, s, fs.tsum, T, fs.tpre));
     MB_LAUNCH_CHECK();
-    k_fold_count<<<nt, kDescThreads, 0, s>>>(x, n, s0, fs.tsum, fs.tpre, T, fs.tq, fs.tw, fs.desc, fs.elast,
-        fs.loc);
+    MB_CUDA(launch_pdl(k_fold_count, nt, kDescThreads, 0, s, x, n, s0, fs.tsum, fs.tpre, T, fs.tq, fs.tw, fs.desc, fs.elast,
+        fs.loc));
     MB_LAUNCH_CHECK();
-    k_fold_scan_counts<<<1, 1024, 0, s>>>(fs.tq, fs.tw, T, fs.pq, fs.pw, fs.tot);
+    MB_CUDA(launch_pdl(k_fold_scan_counts, 1, 1024, 0, s, fs.tq, fs.tw, T, fs.pq, fs.pw, fs.tot));
     MB_LAUNCH_CHECK();
-    k_fold_emit<<<nt, kDescThreads, 0, s>>>(x, n, s0, fs.tpre, T, fs.pq, fs.pw, fs.tw, fs.tot, fs.win, fs.loc);
+    MB_CUDA(launch_pdl(k_fold_emit, nt, kDescThreads, 0, s, x, n, s0, fs.tpre, T, fs.pq, fs.pw, fs.tw, fs.tot, fs.win, fs.loc));
     MB_LAUNCH_CHECK();
-    k_fold_walk<<<1, kWalkThreads, 0, s>>>(x, n, s0, fs.desc, T, fs.tstart, fs.tmode, prefix, fs.final_v, fs.tot,
-        fs.elast, fs.win, fs.mode);
+    MB_CUDA(launch_pdl(k_fold_walk, 1, kWalkThreads, 0, s, x, n, s0, fs.desc, T, fs.tstart, fs.tmode, prefix, fs.final_v, fs.tot,
+        fs.elast, fs.win, fs.mode));
     MB_LAUNCH_CHECK();
     if (prefix) {
-        k_fold_expand<<<nt, kDescThreads, 0, s>>>(x, n, s0, fs.tpre, T, fs.pq, fs.pw, fs.win, fs.mode, fs.desc,
-            fs.tstart, fs.tmode, prefix);
+        MB_CUDA(launch_pdl(k_fold_expand, nt, kDescThreads, 0, s, x, n, s0, fs.tpre, T, fs.pq, fs.pw, fs.win, fs.mode, fs.desc,
+            fs.tstart, fs.tmode, prefix));
         MB_LAUNCH_CHECK();
     }
     return MCKL_B200_OK;

@@ -24,6 +24,7 @@ namespace {
 
 __global__ void k_fill(uint64_t n, double *a, double v)
 {
+    pdl_wait();
     for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         a[i] = v;
@@ -49,6 +50,7 @@ __global__ void k_ar1_propagate(uint64_t n, double *x, const double *eps, double
 __global__ void k_ar1_propagate_dev(uint64_t n, double *x, const double *eps, const double *y, const int *t_dev,
     double phi, double sx, double lconst, double hinv, double *ll)
 {
+    pdl_wait();
     const double yt = y[*t_dev];
     for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
@@ -63,6 +65,7 @@ __global__ void k_ar1_propagate_dev(uint64_t n, double *x, const double *eps, co
 
 __global__ void k_step_inc(int *t_dev)
 {
+    pdl_wait();
     *t_dev += 1;
 }
 
@@ -248,8 +251,8 @@ extern "C" int mckl_b200_pf_ar1_plain_f64(size_t N, size_t T, const double *y, d
             rc = capture(&ga[k].e, [&](cudaStream_t c) {
                 k_step_inc<<<1, 1, 0, c>>>(t_dev);
                 MB_LAUNCH_CHECK();
-                k_ar1_propagate_dev<<<grid_of(N), 256, 0, c>>>(N, x_dev, epsb[k], y_dev, t_dev, phi, sx, lconst, hinv,
-                    ll);
+                MB_CUDA(launch_pdl(k_ar1_propagate_dev, grid_of(N), 256, 0, c, N, x_dev, epsb[k], y_dev, t_dev, phi, sx, lconst, hinv,
+                    ll));
                 MB_LAUNCH_CHECK();
                 int r = weight_normalize_dev(N, W_dev, ll, 1, wscr, wres, c, 0, &fork.f);
                 if (r != MCKL_B200_OK) return r;

@@ -168,6 +168,7 @@ __device__ __forceinline__ double next_down(double v)
 __global__ void k_rep_counts(uint64_t N, uint64_t M, const double *c, const double *u, uint64_t *rep,
     unsigned long long *ties)
 {
+    pdl_wait();
     __shared__ unsigned long long sh[33];
     unsigned long long nt = 0;
     // the bound below c[i - 1] is the previous lane's bound below c[i]: one
@@ -225,6 +226,7 @@ __global__ void k_add_integ(uint64_t N, uint64_t *rep, const uint64_t *integ)
 
 __global__ void k_fill_rep(uint64_t N, uint64_t M, uint64_t *rep)
 {
+    pdl_wait();
     GRID_LOOP(i, N) { rep[i] = (N == 1) ? M : 0; }
 }
 
@@ -266,6 +268,7 @@ __global__ void __launch_bounds__(kScanThreads) k_rep_scan(uint64_t N, uint64_t 
     uint32_t *ex_empty, uint32_t *ex_surplus, unsigned long long *status, unsigned *tile_counter, int *err,
     uint64_t G, uint32_t *coarse)
 {
+    pdl_wait();
     __shared__ unsigned long long sh[33];
     __shared__ unsigned shu[33];
     __shared__ unsigned long long sv[kScanTile + kScanTile / 16];
@@ -362,6 +365,7 @@ __global__ void __launch_bounds__(kScanThreads) k_rep_scan(uint64_t N, uint64_t 
 __global__ void k_rep_place(uint64_t N, uint64_t M, uint64_t K, const uint64_t *rep, const uint32_t *ex_empty,
     uint64_t *idx, uint32_t *empty_pos)
 {
+    pdl_wait();
     const uint64_t n_empty_k = (K == 0) ? 0 : ex_empty[K - 1] + (rep[K - 1] == 0 ? 1 : 0);
     GRID_LOOP(d, M)
     {
@@ -411,6 +415,7 @@ __global__ void __launch_bounds__(kFillThreads) k_rep_fill(uint64_t N, uint64_t 
     const uint32_t *ex_empty, const uint32_t *ex_surplus, const uint32_t *empty_pos, uint64_t G,
     const uint32_t *coarse, uint64_t *idx)
 {
+    pdl_wait();
     __shared__ uint32_t sx[kFillStage];
     __shared__ uint32_t sc[kCoarse];
     __shared__ unsigned sh_b[2];
@@ -467,6 +472,7 @@ __global__ void __launch_bounds__(kFillThreads) k_rep_fill(uint64_t N, uint64_t 
 template <typename T>
 __global__ void k_select_inplace(uint64_t N, uint64_t dim, const uint64_t *idx, T *state)
 {
+    pdl_wait();
     GRID_LOOP(i, N)
     {
         const uint64_t src = idx[i];
@@ -478,6 +484,7 @@ __global__ void k_select_inplace(uint64_t N, uint64_t dim, const uint64_t *idx, 
 template <typename T>
 __global__ void k_select_copy(uint64_t N, uint64_t M, uint64_t dim, const uint64_t *idx, const T *in, T *out)
 {
+    pdl_wait();
     GRID_LOOP(i, M)
     {
         const uint64_t src = idx[i];
@@ -599,12 +606,12 @@ int resample_dev(int scheme, uint64_t N, uint64_t M, mckl_b200_engine_t &e, cons
     int rc = u01_sequence_dev(seq, e, R, u, tmp, fs, s);
     if (rc != MCKL_B200_OK) return rc;
     if (N <= 1 || R == 0) {
-        k_fill_rep<<<cap_grid(N, 256), 256, 0, s>>>(N, R, rep);
+        MB_CUDA(launch_pdl(k_fill_rep, cap_grid(N, 256), 256, 0, s, N, R, rep));
         MB_LAUNCH_CHECK();
     } else {
         rc = fold_exact(weights, N - 1, 0.0, tmp, fs, s);  // cumulative weights of particles 0..N-2
         if (rc != MCKL_B200_OK) return rc;
-        k_rep_counts<<<cap_grid(N, 256), 256, 0, s>>>(N, R, tmp, u, rep, ties_dev);
+        MB_CUDA(launch_pdl(k_rep_counts, cap_grid(N, 256), 256, 0, s, N, R, tmp, u, rep, ties_dev));
         MB_LAUNCH_CHECK();
     }
     if (scheme >= 3) {
@@ -629,13 +636,13 @@ int rep_counts_dev(uint64_t N, uint64_t M, const double *W, const double *u, uin
     cudaStream_t s, unsigned long long *ties_dev)
 {
     if (N <= 1 || M == 0) {
-        k_fill_rep<<<cap_grid(N, 256), 256, 0, s>>>(N, M, rep);
+        MB_CUDA(launch_pdl(k_fill_rep, cap_grid(N, 256), 256, 0, s, N, M, rep));
         MB_LAUNCH_CHECK();
         return MCKL_B200_OK;
     }
     int rc = fold_exact(W, N - 1, 0.0, rs.tmp, rs.fs, s);  // cumulative weights of particles 0..N-2
     if (rc != MCKL_B200_OK) return rc;
-    k_rep_counts<<<cap_grid(N, 256), 256, 0, s>>>(N, M, rs.tmp, u, rep, ties_dev);
+    MB_CUDA(launch_pdl(k_rep_counts, cap_grid(N, 256), 256, 0, s, N, M, rs.tmp, u, rep, ties_dev));
     MB_LAUNCH_CHECK();
     return MCKL_B200_OK;
 }
@@ -670,10 +677,10 @@ int rep_to_index_dev(uint64_t N, uint64_t M, const uint64_t *rep, uint64_t *idx,
     k_rep_scan<<<static_cast<unsigned>(tiles), kScanThreads, 0, s>>>(N, K, rep, ex_empty, ex_surplus, status,
         tile_counter, err_dev, G, coarse);
     MB_LAUNCH_CHECK();
-    k_rep_place<<<cap_grid(M, 256), 256, 0, s>>>(N, M, K, rep, ex_empty, idx, empty_pos);
+    MB_CUDA(launch_pdl(k_rep_place, cap_grid(M, 256), 256, 0, s, N, M, K, rep, ex_empty, idx, empty_pos));
     MB_LAUNCH_CHECK();
-    k_rep_fill<<<cap_grid(M, kFillThreads, 8), kFillThreads, 0, s>>>(N, M, K, rep, ex_empty, ex_surplus, empty_pos,
-        G, coarse, idx);
+    MB_CUDA(launch_pdl(k_rep_fill, cap_grid(M, kFillThreads, 8), kFillThreads, 0, s, N, M, K, rep, ex_empty, ex_surplus, empty_pos,
+        G, coarse, idx));
     MB_LAUNCH_CHECK();
     return MCKL_B200_OK;
 }

@@ -27,6 +27,7 @@ constexpr int kChunk = 1024;  // BufferSize<double> (internal/traits.hpp:171-175
 
 __global__ void k_weight_prep(uint64_t N, double *W, const double *v, int add_log, long long *lmax_bits)
 {
+    pdl_wait();
     __shared__ double sh[33];
     double m = -__longlong_as_double(0x7ff0000000000000ll);
     for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < N;
@@ -47,6 +48,7 @@ __global__ void k_weight_prep(uint64_t N, double *W, const double *v, int add_lo
 
 __global__ void k_weight_exp(uint64_t N, double *W, const long long *lmax_bits)
 {
+    pdl_wait();
     const double lmax = from_ordered_bits(*lmax_bits);
     for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < N;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
@@ -61,6 +63,7 @@ constexpr int kDotWarps = 4;
 
 __global__ void __launch_bounds__(32 * kDotWarps) k_weight_chunkdot(uint64_t N, const double *W, double *dots)
 {
+    pdl_wait();
     __shared__ double sq[kDotWarps][kChunk];
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t c = static_cast<uint64_t>(blockIdx.x) * kDotWarps + warp;
@@ -85,6 +88,7 @@ constexpr int kFinishThreads = 256, kFinishTile = 2048;
 
 __global__ void __launch_bounds__(kFinishThreads) k_weight_dotsum(uint64_t nchunks, const double *dots, double *essw)
 {
+    pdl_wait();
     __shared__ double tile[kFinishTile];
     double acc = 0.0;
     for (uint64_t t0 = 0; t0 < nchunks; t0 += kFinishTile) {
@@ -101,6 +105,7 @@ __global__ void __launch_bounds__(kFinishThreads) k_weight_dotsum(uint64_t nchun
 __global__ void k_weight_finish(const double *essw, const double *accw, const long long *lmax_bits,
     double *out /* [ess, log_nc, accw, lmax] */)
 {
+    pdl_wait();
     const double a = *accw;
     const double lmax = from_ordered_bits(*lmax_bits);
     out[0] = __ddiv_rn(__dmul_rn(a, a), *essw);
@@ -111,11 +116,13 @@ __global__ void k_weight_finish(const double *essw, const double *accw, const lo
 
 __global__ void k_weight_reset(long long *lmax_bits, long long v)
 {
+    pdl_wait();
     *lmax_bits = v;
 }
 
 __global__ void k_weight_scale(uint64_t N, double *W, const double *accw)
 {
+    pdl_wait();
     const double inv = __ddiv_rn(1.0, *accw);
     for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < N;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
@@ -148,11 +155,11 @@ int weight_normalize_dev(uint64_t N, double *W, const double *v, int add_log, vo
     FoldScratch fs = fold_scratch_carve(p + 256 + align256(nchunks * sizeof(double)), N, wcap);
     // the running maximum starts at -inf (a kernel, not a host copy: nothing
     // here reads host memory, so the sequence can be captured in a graph)
-    k_weight_reset<<<1, 1, 0, s>>>(lmax_bits, ordered_bits(-__builtin_huge_val()));
+    MB_CUDA(launch_pdl(k_weight_reset, 1, 1, 0, s, lmax_bits, ordered_bits(-__builtin_huge_val())));
     MB_LAUNCH_CHECK();
-    k_weight_prep<<<grid_cap(N, 256), 256, 0, s>>>(N, W, v, add_log, lmax_bits);
+    MB_CUDA(launch_pdl(k_weight_prep, grid_cap(N, 256), 256, 0, s, N, W, v, add_log, lmax_bits));
     MB_LAUNCH_CHECK();
-    k_weight_exp<<<grid_cap(N, 256), 256, 0, s>>>(N, W, lmax_bits);
+    MB_CUDA(launch_pdl(k_weight_exp, grid_cap(N, 256), 256, 0, s, N, W, lmax_bits));
     MB_LAUNCH_CHECK();
     cudaStream_t ds = s;  // the stream of the ESS's dot products
     if (fork) {
@@ -160,18 +167,29 @@ int weight_normalize_dev(uint64_t N, double *W, const double *v, int add_log, vo
         MB_CUDA(cudaStreamWaitEvent(fork->side, fork->fork, 0));
         ds = fork->side;
     }
-    k_weight_chunkdot<<<static_cast<unsigned>((nchunks + kDotWarps - 1) / kDotWarps), 32 * kDotWarps, 0, ds>>>(N,
-        W, dots);
-    MB_LAUNCH_CHECK();
-    k_weight_dotsum<<<1, kFinishThreads, 0, ds>>>(nchunks, dots, essw);
-    MB_LAUNCH_CHECK();
+    const unsigned ndot = static_cast<unsigned>((nchunks + kDotWarps - 1) / kDotWarps);
+    if (fork) {  // after an event wait: ordinary launches
+        k_weight_chunkdot<<<ndot, 32 * kDotWarps, 0, ds>>>(N, W, dots);
+        MB_LAUNCH_CHECK();
+        k_weight_dotsum<<<1, kFinishThreads, 0, ds>>>(nchunks, dots, essw);
+        MB_LAUNCH_CHECK();
+    } else {
+        MB_CUDA(launch_pdl(k_weight_chunkdot, ndot, 32 * kDotWarps, 0, s, N, W, dots));
+        MB_LAUNCH_CHECK();
+        MB_CUDA(launch_pdl(k_weight_dotsum, 1, kFinishThreads, 0, s, nchunks, dots, essw));
+        MB_LAUNCH_CHECK();
+    }
     if (fork) MB_CUDA(cudaEventRecord(fork->join, fork->side));
     int rc = fold_exact(W, N, 0.0, nullptr, fs, s);
     if (rc != MCKL_B200_OK) return rc;
-    if (fork) MB_CUDA(cudaStreamWaitEvent(s, fork->join, 0));
-    k_weight_finish<<<1, 1, 0, s>>>(essw, fs.final_v, lmax_bits, result_dev);
+    if (fork) {
+        MB_CUDA(cudaStreamWaitEvent(s, fork->join, 0));
+        k_weight_finish<<<1, 1, 0, s>>>(essw, fs.final_v, lmax_bits, result_dev);
+    } else {
+        MB_CUDA(launch_pdl(k_weight_finish, 1, 1, 0, s, essw, fs.final_v, lmax_bits, result_dev));
+    }
     MB_LAUNCH_CHECK();
-    k_weight_scale<<<grid_cap(N, 256), 256, 0, s>>>(N, W, fs.final_v);
+    MB_CUDA(launch_pdl(k_weight_scale, grid_cap(N, 256), 256, 0, s, N, W, fs.final_v));
     MB_LAUNCH_CHECK();
     return MCKL_B200_OK;
 }
