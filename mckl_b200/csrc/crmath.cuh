@@ -36,14 +36,6 @@
 #else
 #define MB_HD inline
 #endif
-// The accurate phases behind a quick phase run for a few arguments in a
-// thousand: kept out of line on the device, so that they do not add to the
-// register pressure of the kernels that inline the quick phase.
-#if defined(__CUDACC__)
-#define MB_HD_COLD inline __host__ __device__ __noinline__
-#else
-#define MB_HD_COLD inline
-#endif
 
 #if defined(__CUDA_ARCH__)
 #define MB_ADD(a, b) __dadd_rn((a), (b))
@@ -233,9 +225,8 @@ MB_HD double scale2(double y, int k)
 
 // The accurate phase of exp: the double-double evaluation below, correctly
 // rounded (see header) for normal results; results in the subnormal range are
-// rounded twice.  exp_dd_inline is the same evaluation inlined (for kernels
-// that call it on every value and measured faster so).
-MB_HD double exp_dd_inline(double x)
+// rounded twice.
+MB_HD double exp_dd(double x)
 {
     if (x != x) return x;
     if (x > 709.782712893384) return MB_FROM_BITS(0x7ff0000000000000ll);
@@ -267,11 +258,6 @@ MB_HD double exp_dd_inline(double x)
     }
     const DD res = add_d(E, 1.0);
     return scale2(MB_ADD(res.hi, res.lo), k);
-}
-
-MB_HD_COLD double exp_dd(double x)
-{
-    return exp_dd_inline(x);
 }
 
 // Table of the quick phase: {hi, lo} of 2^(j/64), j = 0..63 (exp_table.inc,
@@ -367,8 +353,8 @@ constexpr double kPio2P4 = 0x1.129024e088a68p-123;
 
 // The accurate phase of sincos: sin and cos of a double in double-double,
 // correctly rounded (see header) for |x| < 1e5; larger arguments fall back to
-// the device library.  sincos_dd_inline is the same evaluation inlined.
-MB_HD void sincos_dd_inline(double x, double *sp, double *cp)
+// the device library.
+MB_HD void sincos_dd(double x, double *sp, double *cp)
 {
     if (!(x < 1e5 && x > -1e5)) {
         MB_LIB_SINCOS(x, sp, cp);
@@ -419,11 +405,6 @@ MB_HD void sincos_dd_inline(double x, double *sp, double *cp)
         case 2: *sp = -s; *cp = -c; break;
         default: *sp = -c; *cp = s; break;
     }
-}
-
-MB_HD_COLD void sincos_dd(double x, double *sp, double *cp)
-{
-    sincos_dd_inline(x, sp, cp);
 }
 
 // Table of the quick phase: {sin hi, lo, cos hi, lo} of j/64, j = 0..51

@@ -50,12 +50,9 @@ struct GOps<double> {
     __device__ static double div(double a, double b) { return __ddiv_rn(a, b); }
     __device__ static double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
     __device__ static double log(double a) { return dd::log(a); }
-    // the double-double evaluations inlined, without the quick phases: with
-    // them (and the accurate phases out of line) the algorithm-N kernels
-    // spill more and measured 5 % slower
-    __device__ static double exp(double a) { return dd::exp_dd_inline(a); }
+    __device__ static double exp(double a) { return dd::exp(a); }
     __device__ static double sqrt(double a) { return __dsqrt_rn(a); }
-    __device__ static void sincos(double a, double *s, double *c) { dd::sincos_dd_inline(a, s, c); }
+    __device__ static void sincos(double a, double *s, double *c) { dd::sincos(a, s, c); }
 };
 
 template <>
