@@ -21,6 +21,41 @@ __device__ __forceinline__ double ulp_of(double v)
     return grid_unit(eb);
 }
 
+// Maximum of nonnegative doubles over the CTA (0 for none): the total, and
+// the maximum over the threads before this one.  `sh` needs 33 elements.
+__device__ __forceinline__ double block_exclusive_max(double v, double *sh, double *total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc = fmax(inc, u);
+    }
+    double prev = __shfl_up_sync(0xffffffffu, inc, 1);
+    if (lane == 0) prev = 0.0;
+    if (lane == 31) sh[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        double w = lane < nw ? sh[lane] : 0.0;
+        double wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double u = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi = fmax(wi, u);
+        }
+        double we = __shfl_up_sync(0xffffffffu, wi, 1);
+        if (lane == 0) we = 0.0;
+        if (lane < nw) sh[lane] = we;
+        if (lane == nw - 1) sh[32] = wi;
+    }
+    __syncthreads();
+    const double r = warp > 0 ? fmax(sh[warp], prev) : prev;
+    *total = sh[32];
+    __syncthreads();
+    return r;
+}
+
 
 // ---------------------------------------------------------------------------
 // Approximate partial sums and the classification of every element.
@@ -33,32 +68,98 @@ __device__ __forceinline__ double ulp_of(double v)
 // 2 (j + 1) + 2 T + 160 ulps of A_j holds S_j with room to spare: when
 // [A_j - margin, A_j + margin] lies inside one binade, S_j certainly does.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int certain_binade(double A, uint64_t j, uint64_t T)
+//
+// Below 2^-1021 (biased exponent 0 or 1) every sum is exact: all partial
+// sums of nonnegative terms are at most the total, and any sum of multiples
+// of 2^-1074 below 2^-1021 is representable.  A tree sum below 2^-1021 is
+// therefore the exact sum, which the sequential fold also reaches, and its
+// binade is certain (this includes zero sums).
+//
+// The sequential fold never decreases and rounds monotonically, so S_j is at
+// least the largest term so far, M_j: the lower end is max(A - margin, M_j).
+// Where one term dominates -- degenerate weights, whose largest term is
+// exactly 1 = 2^0 with a tiny remainder -- the sum sits just above a binade
+// boundary that the margin alone would straddle.
+__device__ __forceinline__ int certain_binade(double A, uint64_t j, uint64_t T, double M)
 {
+    if (biased_exp(A) <= 1 && A >= 0.0) return biased_exp(A);
     const double m = (2.0 * static_cast<double>(j + 1) + 2.0 * static_cast<double>(T) + 160.0) * ulp_of(A);
-    const double lo = __dsub_rn(A, m), hi = __dadd_rn(A, m);
+    const double lo = fmax(__dsub_rn(A, m), M), hi = __dadd_rn(A, m);
     if (!(lo > 0.0)) return -1;
     const int e = biased_exp(lo);
     if (e == 0x7ff || biased_exp(hi) != e) return -1;
     return e;
 }
 
+// One CTA scan of (sum, maximum) pairs: the exclusive sum (formed without a
+// subtraction, as block_exclusive_sum) and the exclusive maximum (0 for
+// none).  `shs`, `shm` need 33 elements each.
+__device__ __forceinline__ void block_exclusive_sum_max(double v, double m, double *shs, double *shm,
+    double *ex_s, double *ex_m)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double is = v, im = m;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double us = __shfl_up_sync(0xffffffffu, is, o);
+        const double um = __shfl_up_sync(0xffffffffu, im, o);
+        if (lane >= o) {
+            is += us;
+            im = fmax(im, um);
+        }
+    }
+    double ps = __shfl_up_sync(0xffffffffu, is, 1), pm = __shfl_up_sync(0xffffffffu, im, 1);
+    if (lane == 0) ps = pm = 0.0;
+    if (lane == 31) {
+        shs[warp] = is;
+        shm[warp] = im;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        double ws = lane < nw ? shs[lane] : 0.0, wm = lane < nw ? shm[lane] : 0.0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double us = __shfl_up_sync(0xffffffffu, ws, o);
+            const double um = __shfl_up_sync(0xffffffffu, wm, o);
+            if (lane >= o) {
+                ws += us;
+                wm = fmax(wm, um);
+            }
+        }
+        double es = __shfl_up_sync(0xffffffffu, ws, 1), em = __shfl_up_sync(0xffffffffu, wm, 1);
+        if (lane == 0) es = em = 0.0;
+        if (lane < nw) {
+            shs[lane] = es;
+            shm[lane] = em;
+        }
+    }
+    __syncthreads();
+    *ex_s = warp > 0 ? shs[warp] + ps : ps;
+    *ex_m = warp > 0 ? fmax(shm[warp], pm) : pm;
+    __syncthreads();
+}
+
 // The tile's kPer elements of this thread (zeros past n), the approximate
-// partial sum before the first of them and their own sum.
-__device__ __forceinline__ void tile_load(const double *x, uint64_t n, double s0, const double *tpre, uint64_t t,
-    double (&xv)[kPer], double *sh, double *Abefore, double *own_sum = nullptr)
+// partial sum before the first of them, their own sum, and the largest term
+// before them (s0 included).
+__device__ __forceinline__ void tile_load(const double *x, uint64_t n, double s0, const double *tpre,
+    const double *tpmax, uint64_t t, double (&xv)[kPer], double *sh, double *Abefore, double *own_sum,
+    double *Mbefore)
 {
     const uint64_t i0 = t * kFoldTile + static_cast<uint64_t>(threadIdx.x) * kPer;
-    double own = 0.0;
+    double own = 0.0, mx = 0.0;
 #pragma unroll
     for (int k = 0; k < kPer; ++k) {
         xv[k] = i0 + k < n ? x[i0 + k] : 0.0;
         own = __dadd_rn(own, xv[k]);
+        mx = fmax(mx, xv[k]);
     }
-    double tot;
-    const double ex = block_exclusive_sum(own, sh, &tot);
+    __shared__ double shm[33];
+    double ex, exm;
+    block_exclusive_sum_max(own, mx, sh, shm, &ex, &exm);
     *Abefore = __dadd_rn(__dadd_rn(s0, tpre[t]), ex);
-    if (own_sum) *own_sum = own;
+    *own_sum = own;
+    *Mbefore = fmax(fmax(s0, tpmax[t]), exm);
 }
 
 // Element j = i0 + k is a RUN element when the binades of S_{j-1} and S_j
@@ -75,13 +176,15 @@ __device__ __forceinline__ void tile_load(const double *x, uint64_t n, double s0
 // every element's binade is certain and the same, and only its increment
 // remains to be checked.
 __device__ __forceinline__ void classify(const double (&xv)[kPer], uint64_t i0, uint64_t n, uint64_t T, double s0,
-    double Abefore, double own, long long (&q)[kPer], unsigned &win, int (&eprev)[kPer], int *fast_e = nullptr)
+    double Abefore, double own, double Mbefore, long long (&q)[kPer], unsigned &win, int (&eprev)[kPer],
+    int *fast_e = nullptr)
 {
     if (fast_e) *fast_e = -1;
     {
         const double Aend = __dadd_rn(Abefore, own);
         const double c = 2.0 * static_cast<double>(i0 + kPer) + 2.0 * static_cast<double>(T) + 160.0;
-        const double lo = __dsub_rn(Abefore, c * ulp_of(Abefore)), hi = __dadd_rn(Aend, c * ulp_of(Aend));
+        const double lo = fmax(__dsub_rn(Abefore, c * ulp_of(Abefore)), Mbefore);
+        const double hi = __dadd_rn(Aend, c * ulp_of(Aend));
         const int e = biased_exp(lo);
         if (lo > 0.0 && e != 0x7ff && biased_exp(hi) == e) {
             win = 0;
@@ -99,13 +202,15 @@ __device__ __forceinline__ void classify(const double (&xv)[kPer], uint64_t i0, 
             return;
         }
     }
+    // A zero sum lies on the grid of binade 0 (the subnormals'), so a stretch
+    // of leading zeros is a run, not a window per element.
     int ep;
     if (i0 == 0) {
-        ep = (s0 > 0.0 && biased_exp(s0) != 0x7ff) ? biased_exp(s0) : -1;  // s0 itself is exact
+        ep = (s0 >= 0.0 && biased_exp(s0) != 0x7ff) ? biased_exp(s0) : -1;  // s0 itself is exact
     } else {
-        ep = certain_binade(Abefore, i0 - 1, T);
+        ep = certain_binade(Abefore, i0 - 1, T, Mbefore);
     }
-    double A = Abefore;
+    double A = Abefore, M = Mbefore;
     win = 0;
 #pragma unroll
     for (int k = 0; k < kPer; ++k) {
@@ -114,7 +219,13 @@ __device__ __forceinline__ void classify(const double (&xv)[kPer], uint64_t i0, 
         eprev[k] = ep;
         if (j < n) {
             A = __dadd_rn(A, xv[k]);
-            const int ej = certain_binade(A, j, T);
+            M = fmax(M, xv[k]);
+            // a zero term leaves the sum unchanged (S_j = S_{j-1}): it keeps
+            // the previous binade, certain or not, and is never a window; a
+            // run of zeros alone adds nothing, so the walk needs no binade
+            // for it
+            if (xv[k] == 0.0) continue;
+            const int ej = certain_binade(A, j, T, M);
             bool ev = true;
             if (ej >= 0 && ej == ep) q[k] = grid_increment(xv[k], ej, ev);
             if (ev) {
@@ -127,33 +238,50 @@ __device__ __forceinline__ void classify(const double (&xv)[kPer], uint64_t i0, 
 }
 
 // 1. approximate tile sums
-__global__ void __launch_bounds__(kDescThreads) k_fold_tilesum(const double *x, uint64_t n, double *tsum)
+__global__ void __launch_bounds__(kDescThreads) k_fold_tilesum(const double *x, uint64_t n, double *tsum,
+    double *tmax)
 {
     pdl_wait();
     __shared__ double sh[33];
     const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kFoldTile;
-    double acc = 0;
+    double acc = 0, mx = 0;
     for (int k = 0; k < kPer; ++k) {
         const uint64_t i = base + k * kDescThreads + threadIdx.x;
-        if (i < n) acc += x[i];
+        if (i < n) {
+            acc += x[i];
+            mx = fmax(mx, x[i]);
+        }
     }
     acc = block_sum(acc, sh);
-    if (threadIdx.x == 0) tsum[blockIdx.x] = acc;
+    double mt;
+    block_exclusive_max(mx, sh, &mt);
+    if (threadIdx.x == 0) {
+        tsum[blockIdx.x] = acc;
+        tmax[blockIdx.x] = mt;
+    }
 }
 
 // 2. exclusive prefix of the tile sums (one CTA), formed without subtraction
-__global__ void __launch_bounds__(1024) k_fold_scan_tiles(const double *tsum, uint64_t T, double *tpre)
+// (and, in place, the exclusive prefix maximum of the tile maxima)
+__global__ void __launch_bounds__(1024) k_fold_scan_tiles(const double *tsum, uint64_t T, double *tpre,
+    double *tpmax)
 {
     pdl_wait();
     __shared__ double sh[33];
-    double carry = 0;
+    double carry = 0, mcarry = 0;
     for (uint64_t b = 0; b < T; b += blockDim.x) {
         const uint64_t t = b + threadIdx.x;
         const double v = t < T ? tsum[t] : 0.0;
-        double tot;
+        const double mv = t < T ? tpmax[t] : 0.0;
+        double tot, mtot;
         const double ex = block_exclusive_sum(v, sh, &tot);
-        if (t < T) tpre[t] = b == 0 ? ex : carry + ex;
+        const double exm = block_exclusive_max(mv, sh, &mtot);
+        if (t < T) {
+            tpre[t] = b == 0 ? ex : carry + ex;
+            tpmax[t] = fmax(mcarry, exm);
+        }
         carry += tot;
+        mcarry = fmax(mcarry, mtot);
     }
 }
 
@@ -161,7 +289,7 @@ __global__ void __launch_bounds__(1024) k_fold_scan_tiles(const double *tsum, ui
 // tile's window list (when it fits), and the tile descriptor of the
 // event-loop walk (the fallback)
 __global__ void __launch_bounds__(kDescThreads) k_fold_count(const double *x, uint64_t n, double s0,
-    const double *tsum, const double *tpre, uint64_t T, long long *tq, unsigned *tw, FoldDesc *desc, int *elast,
+    const double *tsum, const double *tpre, const double *tpmax, uint64_t T, long long *tq, unsigned *tw, FoldDesc *desc, int *elast,
     FoldLocal loc)
 {
     pdl_wait();
@@ -171,13 +299,13 @@ __global__ void __launch_bounds__(kDescThreads) k_fold_count(const double *x, ui
     const uint64_t t = blockIdx.x;
     const uint64_t base = t * kFoldTile;
     const uint64_t i0 = base + static_cast<uint64_t>(threadIdx.x) * kPer;
-    double xv[kPer], Ab, own;
-    tile_load(x, n, s0, tpre, t, xv, shd, &Ab, &own);
+    double xv[kPer], Ab, own, Mb;
+    tile_load(x, n, s0, tpre, tpmax, t, xv, shd, &Ab, &own, &Mb);
     long long q[kPer];
     unsigned win;
     int ep[kPer];
     int fe;
-    classify(xv, i0, n, T, s0, Ab, own, q, win, ep, &fe);
+    classify(xv, i0, n, T, s0, Ab, own, Mb, q, win, ep, &fe);
     long long qs = 0;
 #pragma unroll
     for (int k = 0; k < kPer; ++k) {
@@ -276,7 +404,7 @@ __global__ void __launch_bounds__(1024) k_fold_scan_counts(const long long *tq, 
 // 5. the windows in order: index, value, run-increment prefix before it and
 // the binade of the run before it
 __global__ void __launch_bounds__(kDescThreads) k_fold_emit(const double *x, uint64_t n, double s0,
-    const double *tpre, uint64_t T, const long long *pq, const unsigned long long *pw, const unsigned *tw,
+    const double *tpre, const double *tpmax, uint64_t T, const long long *pq, const unsigned long long *pw, const unsigned *tw,
     const long long *tot, FoldWindows w, FoldLocal loc)
 {
     pdl_wait();
@@ -298,12 +426,12 @@ __global__ void __launch_bounds__(kDescThreads) k_fold_emit(const double *x, uin
         return;
     }
     const uint64_t i0 = t * kFoldTile + static_cast<uint64_t>(threadIdx.x) * kPer;
-    double xv[kPer], Ab, own;
-    tile_load(x, n, s0, tpre, t, xv, shd, &Ab, &own);
+    double xv[kPer], Ab, own, Mb;
+    tile_load(x, n, s0, tpre, tpmax, t, xv, shd, &Ab, &own, &Mb);
     long long q[kPer];
     unsigned win;
     int ep[kPer];
-    classify(xv, i0, n, T, s0, Ab, own, q, win, ep);
+    classify(xv, i0, n, T, s0, Ab, own, Mb, q, win, ep);
     long long qs = 0;
 #pragma unroll
     for (int k = 0; k < kPer; ++k) qs += q[k];
@@ -593,9 +721,9 @@ __global__ void __launch_bounds__(kWalkThreads) k_fold_walk(const double *x, uin
             unsigned long long jn = sh_j;
             int good = 1;
             for (unsigned k = 0; k < m; ++k) {
-                if (sj[k] > jn) {  // the run jn .. sj[k] - 1
+                if (sj[k] > jn && sp[k] != p) {  // the run jn .. sj[k] - 1 (a zero sum is on binade 0's grid)
                     const int e = se[k];
-                    if (!(s > 0.0) || biased_exp(s) != e) {
+                    if (!(s >= 0.0) || biased_exp(s) != e) {
                         good = 0;
                         break;
                     }
@@ -620,10 +748,10 @@ __global__ void __launch_bounds__(kWalkThreads) k_fold_walk(const double *x, uin
     }
     if (threadIdx.x == 0 && sh_ok) {
         double s = sh_s;
-        if (sh_j < n) {  // the run after the last window
+        if (sh_j < n && sh_q != sh_p) {  // the run after the last window, when it adds anything
             const int e = sh_elast;
             const long long K = grid_count(s) + (sh_q - sh_p);
-            if (e < 0 || !(s > 0.0) || biased_exp(s) != e || K >= grid_top(e)) {
+            if (e < 0 || !(s >= 0.0) || biased_exp(s) != e || K >= grid_top(e)) {
                 sh_ok = 0;
             } else {
                 s = from_grid(K, e);
@@ -645,7 +773,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_fold_walk(const double *x, uin
 // value after the window before it plus its run's increments on the grid, a
 // window element the walk's value.
 __global__ void __launch_bounds__(kDescThreads) k_fold_expand(const double *x, uint64_t n, double s0,
-    const double *tpre, uint64_t T, const long long *pq, const unsigned long long *pw, FoldWindows w,
+    const double *tpre, const double *tpmax, uint64_t T, const long long *pq, const unsigned long long *pw, FoldWindows w,
     const int *mode, const FoldDesc *desc, const double *tstart, const int *tmode, double *prefix)
 {
     pdl_wait();
@@ -658,12 +786,12 @@ __global__ void __launch_bounds__(kDescThreads) k_fold_expand(const double *x, u
         return;
     }
     const uint64_t i0 = t * kFoldTile + static_cast<uint64_t>(threadIdx.x) * kPer;
-    double xv[kPer], Ab, own;
-    tile_load(x, n, s0, tpre, t, xv, shd, &Ab, &own);
+    double xv[kPer], Ab, own, Mb;
+    tile_load(x, n, s0, tpre, tpmax, t, xv, shd, &Ab, &own, &Mb);
     long long q[kPer];
     unsigned win;
     int ep[kPer];
-    classify(xv, i0, n, T, s0, Ab, own, q, win, ep);
+    classify(xv, i0, n, T, s0, Ab, own, Mb, q, win, ep);
     long long qs = 0;
 #pragma unroll
     for (int k = 0; k < kPer; ++k) qs += q[k];
@@ -705,7 +833,7 @@ size_t fold_scratch_bytes(uint64_t n, uint64_t wcap)
     const uint64_t T = (n + kFoldTile - 1) / kFoldTile + 1;
     const uint64_t L = wcap == 0 ? T * kFoldLocalCap : 0;
     if (wcap == 0) wcap = fold_window_cap(n);
-    return align256(T * sizeof(FoldDesc)) + 3 * align256(T * sizeof(double)) + align256(T * sizeof(int)) +
+    return align256(T * sizeof(FoldDesc)) + 4 * align256(T * sizeof(double)) + align256(T * sizeof(int)) +
            align256(T * sizeof(long long)) + align256(T * sizeof(unsigned)) + align256(T * sizeof(long long)) +
            align256(T * sizeof(unsigned long long)) + 256 + align256(wcap * sizeof(unsigned long long)) +
            3 * align256(wcap * sizeof(double)) + align256(wcap * sizeof(int)) + 2 * align256(L * sizeof(int)) +
@@ -727,6 +855,7 @@ FoldScratch fold_scratch_carve(void *base, uint64_t n, uint64_t wcap)
     f.desc = reinterpret_cast<FoldDesc *>(take(T * sizeof(FoldDesc)));
     f.tsum = reinterpret_cast<double *>(take(T * sizeof(double)));
     f.tpre = reinterpret_cast<double *>(take(T * sizeof(double)));
+    f.tpmax = reinterpret_cast<double *>(take(T * sizeof(double)));
     f.tstart = reinterpret_cast<double *>(take(T * sizeof(double)));
     f.tmode = reinterpret_cast<int *>(take(T * sizeof(int)));
     f.tq = reinterpret_cast<long long *>(take(T * sizeof(long long)));
@@ -762,23 +891,24 @@ int fold_exact(const double *x, uint64_t n, double s0, double *prefix, FoldScrat
     }
     const uint64_t T = (n + kFoldTile - 1) / kFoldTile;
     const unsigned nt = static_cast<unsigned>(T);
-    MB_CUDA(launch_pdl(k_fold_tilesum, nt, kDescThreads, 0, s, x, n, fs.tsum));
+    MB_CUDA(launch_pdl(k_fold_tilesum, nt, kDescThreads, 0, s, x, n, fs.tsum, fs.tpmax));
     MB_LAUNCH_CHECK();
-    MB_CUDA(launch_pdl(k_fold_scan_tiles, 1, 1024, 0, s, fs.tsum, T, fs.tpre));
+    MB_CUDA(launch_pdl(k_fold_scan_tiles, 1, 1024, 0, s, fs.tsum, T, fs.tpre, fs.tpmax));
     MB_LAUNCH_CHECK();
-    MB_CUDA(launch_pdl(k_fold_count, nt, kDescThreads, 0, s, x, n, s0, fs.tsum, fs.tpre, T, fs.tq, fs.tw, fs.desc, fs.elast,
-        fs.loc));
+    MB_CUDA(launch_pdl(k_fold_count, nt, kDescThreads, 0, s, x, n, s0, fs.tsum, fs.tpre, fs.tpmax, T, fs.tq, fs.tw,
+        fs.desc, fs.elast, fs.loc));
     MB_LAUNCH_CHECK();
     MB_CUDA(launch_pdl(k_fold_scan_counts, 1, 1024, 0, s, fs.tq, fs.tw, T, fs.pq, fs.pw, fs.tot));
     MB_LAUNCH_CHECK();
-    MB_CUDA(launch_pdl(k_fold_emit, nt, kDescThreads, 0, s, x, n, s0, fs.tpre, T, fs.pq, fs.pw, fs.tw, fs.tot, fs.win, fs.loc));
+    MB_CUDA(launch_pdl(k_fold_emit, nt, kDescThreads, 0, s, x, n, s0, fs.tpre, fs.tpmax, T, fs.pq, fs.pw, fs.tw,
+        fs.tot, fs.win, fs.loc));
     MB_LAUNCH_CHECK();
-    MB_CUDA(launch_pdl(k_fold_walk, 1, kWalkThreads, 0, s, x, n, s0, fs.desc, T, fs.tstart, fs.tmode, prefix, fs.final_v, fs.tot,
-        fs.elast, fs.win, fs.mode));
+    MB_CUDA(launch_pdl(k_fold_walk, 1, kWalkThreads, 0, s, x, n, s0, fs.desc, T, fs.tstart, fs.tmode, prefix,
+        fs.final_v, fs.tot, fs.elast, fs.win, fs.mode));
     MB_LAUNCH_CHECK();
     if (prefix) {
-        MB_CUDA(launch_pdl(k_fold_expand, nt, kDescThreads, 0, s, x, n, s0, fs.tpre, T, fs.pq, fs.pw, fs.win, fs.mode, fs.desc,
-            fs.tstart, fs.tmode, prefix));
+        MB_CUDA(launch_pdl(k_fold_expand, nt, kDescThreads, 0, s, x, n, s0, fs.tpre, fs.tpmax, T, fs.pq, fs.pw,
+            fs.win, fs.mode, fs.desc, fs.tstart, fs.tmode, prefix));
         MB_LAUNCH_CHECK();
     }
     return MCKL_B200_OK;

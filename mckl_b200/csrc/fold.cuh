@@ -149,6 +149,7 @@ struct FoldLocal {
 struct FoldScratch {
     double *tsum;     // [T] approximate tile sums
     double *tpre;     // [T] approximate exclusive prefix of tile sums
+    double *tpmax;    // [T] tile maxima, then their exclusive prefix maximum
     FoldDesc *desc;   // [T] tile descriptors of the event-loop walk
     double *tstart;   // [T] event-loop walk: exact value entering each tile
     int *tmode;       // [T] event-loop walk: 0 expand from tstart, 1 values already written

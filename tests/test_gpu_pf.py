@@ -75,3 +75,28 @@ def test_pf_full_size_against_kalman(env):
     want = orc.pf_ar1(N, y30, 0.9, 1.0, 0.5, SD0, (11, 0), (12, 0), 2)
     res30 = mb.pf_ar1_plain(N, y30, 0.9, 1.0, 0.5, SD0, (11, 0), (12, 0), scheme=2, record=True)
     assert compare(res30, want, N) == 0
+
+
+@pytest.mark.parametrize("scheme", [2, 0])
+def test_pf_degenerate_weights_vs_oracle(env, scheme):
+    """Observation outliers collapse the weights in one step (ESS near 1): the
+    resampling then works on cumulative weights with one term just below 1
+    and almost all others zero, and a run without resampling (threshold 0)
+    drives the weights degenerate over many steps.  Decisions, ancestors,
+    ESS and log-likelihood against the oracle, as in the other runs."""
+    mb, orc = env
+    _, y = orc.simulate_ar1(60, 0.9, 1.0, 0.5, SD0, (8, 0))
+    y = y.copy()
+    y[12] += 25.0
+    y[31] -= 40.0
+    y[47] += 15.0
+    N = 1 << 14
+    want = orc.pf_ar1(N, y, 0.9, 1.0, 0.5, SD0, (11, 0), (12, 0), scheme)
+    res = mb.pf_ar1_plain(N, y, 0.9, 1.0, 0.5, SD0, (11, 0), (12, 0), scheme=scheme, record=True)
+    assert res["resampled"][[12, 31, 47]].all()
+    assert compare(res, want, N) == 0
+    want0 = orc.pf_ar1(N, y, 0.9, 1.0, 0.5, SD0, (11, 0), (12, 0), scheme, threshold=0.0)
+    res0 = mb.pf_ar1_plain(N, y, 0.9, 1.0, 0.5, SD0, (11, 0), (12, 0), scheme=scheme, threshold=0.0, record=True)
+    assert not res0["resampled"].any()
+    assert compare(res0, want0, N) == 0
+

@@ -55,6 +55,34 @@ def fold_inputs():
     big = rng.random(70000)
     big[::7000] = 1e6
     out.append(("spikes", big))
+    # leading zeros (a zero running sum is exact): degenerate weights, a
+    # run of zeros before the first positive value, zeros then subnormals
+    lead = rng.random(300000)
+    lead[:250000] = 0.0
+    out.append(("leading zeros", lead))
+    deg = np.zeros(1 << 20)
+    hit = rng.integers(0, 1 << 20, 40)
+    deg[hit] = np.exp(rng.normal(0, 30, 40))
+    deg[hit[:5]] = 5e-324 * rng.integers(1, 1000, 5)
+    out.append(("degenerate", deg))
+    sub = np.zeros(60000)
+    sub[20000:] = 5e-324 * rng.integers(0, 4, 40000)
+    out.append(("zeros then subnormals", sub))
+    out.append(("all zeros", np.zeros(10000)))
+    # a subnormal running sum followed by zeros and small values, crossing
+    # into the normal range (every sum below 2^-1021 is exact)
+    sn = np.zeros(200000)
+    sn[1000] = 3e-320
+    sn[rng.integers(2000, 200000, 300)] = 5e-324 * rng.integers(1, 2**40, 300)
+    sn[150000] = 1e-300
+    out.append(("subnormal sums", sn))
+    # normalised degenerate weights: one weight just below 1, a few tiny
+    # ones, zeros elsewhere (the cumulative sums stay just below 1)
+    nd = np.zeros(1 << 20)
+    pos = rng.integers(0, 1 << 20, 600)
+    nd[pos] = np.exp(rng.normal(-40, 8, 600))
+    nd[pos[0]] = 1.0
+    out.append(("normalised degenerate", nd * (1.0 / np.cumsum(nd)[-1])))
     return out
 
 
