@@ -417,10 +417,20 @@ def bench_plain_c3(N=1 << 20, T=1000):
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
     kf, _ = kalman_ar1(y, phi, sx, sy)
+    # the same filter with resampling off: the weights degenerate (all but a
+    # few hundred exactly zero), the hard case for the exact folds
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    res0 = mb.pf_ar1_plain(N, y, phi, sx, sy, sd0, (11, 0), (12, 0), scheme=mb.Systematic, threshold=0.0)
+    torch.cuda.synchronize()
+    dt0 = time.perf_counter() - t1
     return {"workload": f"plain FP64 particle filter, N = 2^20, T = {T}, systematic resampling at ESS < N/2",
             "particle_steps_per_s": N * T / dt, "s": round(dt, 3), "resampling_steps": int(res["resampled"].sum()),
             "loglik": res["loglik"], "loglik_minus_kalman": float(res["loglik"] - kf[0]),
             "scan_ties": res["ties"],
+            "no_resampling": {"particle_steps_per_s": N * T / dt0, "s": round(dt0, 3),
+                              "final_ess": float(res0["ess"][-1]),
+                              "note": "threshold 0: the weights degenerate, all but a few exactly zero"},
             "scan_ties_note": "uniforms within one representable step of a cumulative weight, over all resampling "
                               "steps; the cumulative weights are the reference's sequential fold bit for bit, so "
                               "a tie flips no ancestor",
