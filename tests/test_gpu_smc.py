@@ -83,6 +83,13 @@ def fold_inputs():
     nd[pos] = np.exp(rng.normal(-40, 8, 600))
     nd[pos[0]] = 1.0
     out.append(("normalised degenerate", nd * (1.0 / np.cumsum(nd)[-1])))
+    # more windows than the list holds: 1 + 2^-53 is a tie (it rounds back to
+    # 1), so every element after the first is a window and the fold takes
+    # the event loop; appended ordinary values give that loop certain tiles
+    # whose descriptors come from the counting pass
+    tie = np.concatenate([[1.0], np.full(20000, 2.0**-53)])
+    out.append(("ties everywhere", tie))
+    out.append(("ties then values", np.concatenate([tie, rng.random(280000)])))
     return out
 
 
