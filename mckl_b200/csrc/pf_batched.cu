@@ -312,12 +312,19 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_adjoint(const BatchedFilter *
 // per particle and step (proposal index in [0, 2N) and acceptance uniform of
 // each of the eight moves).
 // ---------------------------------------------------------------------------
+// One 32-byte record per particle: the three components of tau, so that a
+// backward draw's tau is one sector
+struct __align__(32) ScoreTau {
+    double a0, a1, a2, pad;
+};
+
 struct ScoreArgs {
     uint64_t nmax;
-    double *xb;            // 2 x nmax per CTA: clouds at t - 1 and t before their resampling
-    double *w;             // nmax per CTA: lw_j = log W_j - log(rep_j + 1) of the cloud at t - 1
+    double *xb;            // nmax per CTA: the cloud at t before its resampling
+    double2 *xw;           // 2 x nmax per CTA: (x_j, lw_j) of the clouds at t - 1 and t, lw_j = log W_j -
+                           // log(rep_j + 1), so that a backward draw reads one 16-byte pair
     uint32_t *rep, *anc;   // nmax per CTA: copies of each particle at t - 1, parent of each slot
-    double *tau;           // 2 x 3 x nmax per CTA (component-major)
+    ScoreTau *tau;         // 2 x nmax per CTA
     double *score;         // 3 per filter
 };
 
@@ -331,10 +338,10 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_score(const BatchedFilter *fi
     __shared__ __align__(16) uint32_t shj[shj_words<THREADS>()];
     __shared__ int sh_f;
     const uint64_t slot = blockIdx.x, nm = A.nmax;
-    double *xbuf[2] = {A.xb + slot * 2 * nm, A.xb + slot * 2 * nm + nm};
-    double *W = A.w + slot * nm;
+    double *xnow = A.xb + slot * nm;
+    double2 *xwb[2] = {A.xw + slot * 2 * nm, A.xw + slot * 2 * nm + nm};
     uint32_t *rep = A.rep + slot * nm, *anc = A.anc + slot * nm;
-    double *taub[2] = {A.tau + slot * 6 * nm, A.tau + slot * 6 * nm + 3 * nm};
+    ScoreTau *taub[2] = {A.tau + slot * 2 * nm, A.tau + slot * 2 * nm + nm};
     while (true) {
         if (threadIdx.x == 0) {
             const int k = atomicAdd(queue, 1);
@@ -359,11 +366,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_score(const BatchedFilter *fi
         for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
             const double x0 = run.xc[p];
             const double v = x0 * x0 * isd02 - 1.0;
-            xbuf[0][p] = x0;
-            W[p] = 0.0;
-            taub[0][p] = v * phi / q0;
-            taub[0][nm + p] = v / sx;
-            taub[0][2 * nm + p] = 0.0;
+            xwb[0][p] = make_double2(x0, 0.0);
+            taub[0][p] = ScoreTau{v * phi / q0, v / sx, 0.0, 0.0};
         }
         __syncthreads();
         int cur = 0;
@@ -371,19 +375,22 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_score(const BatchedFilter *fi
         // their own parents (anc = identity, rep = 1) and the arrays are not read
         bool resampled = false;
         for (int t = 1; t <= T; ++t) {
-            double *xprev = xbuf[(t - 1) & 1], *xnow = xbuf[t & 1];
+            const double2 *xwp = xwb[(t - 1) & 1];
+            double2 *xwn = xwb[t & 1];
             run.rec_x = xnow;  // the step records its cloud before resampling
             const bool res = run.step(t, yf[t], shd, shd, shu, shj);
             run.rec_x = nullptr;
             // PaRIS update of every particle of the cloud at t
-            const double *tp = taub[cur];
-            double *tn = taub[cur ^ 1];
+            const ScoreTau *tp = taub[cur];
+            ScoreTau *tn = taub[cur ^ 1];
             const double yt = yf[t];
             for (uint64_t i = threadIdx.x; i < N; i += THREADS) {
                 const double xi = xnow[i];
                 uint32_t J = resampled ? anc[i] : static_cast<uint32_t>(i);
-                double dJ = xi - phi * xprev[J];
-                double lJ = W[J];
+                const double2 pJ = xwp[J];
+                double xJ = pJ.x;
+                double dJ = xi - phi * xJ;
+                double lJ = pJ.y;
                 double a0 = 0.0, a1 = 0.0, a2 = 0.0;
 #pragma unroll 1
                 for (int b = 0; b < 4; ++b) {
@@ -395,28 +402,28 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_score(const BatchedFilter *fi
                         const uint32_t k =
                             static_cast<uint32_t>((static_cast<uint64_t>(wd[2 * m]) * (2ull * N32)) >> 32);
                         const uint32_t jp = k < N32 ? (resampled ? anc[k] : k) : k - N32;
-                        const double dp = xi - phi * xprev[jp];
-                        const double lp = W[jp];
+                        const double2 pp = xwp[jp];
+                        const double dp = xi - phi * pp.x;
+                        const double lp = pp.y;
                         // log of the acceptance ratio
                         const double lr = (dJ * dJ - dp * dp) * hsx2 + lp - lJ;
                         const double u = (static_cast<double>(wd[2 * m + 1]) + 0.5) * 0x1p-32;
                         if (log(u) < lr) {
                             J = jp;
+                            xJ = pp.x;
                             dJ = dp;
                             lJ = lp;
                         }
                     }
                     if (b == 1 || b == 3) {  // the states after moves 4 and 8
-                        const double xJ = xprev[J];
-                        a0 += tp[J] + dJ * xJ * isx2;
-                        a1 += tp[nm + J] + (dJ * dJ * isx2 - 1.0) / sx;
-                        a2 += tp[2 * nm + J];
+                        const ScoreTau tJ = tp[J];
+                        a0 += tJ.a0 + dJ * xJ * isx2;
+                        a1 += tJ.a1 + (dJ * dJ * isx2 - 1.0) / sx;
+                        a2 += tJ.a2;
                     }
                 }
                 const double r = yt - xi;
-                tn[i] = 0.5 * a0;
-                tn[nm + i] = 0.5 * a1;
-                tn[2 * nm + i] = 0.5 * a2 + (r * r / (sy * sy) - 1.0) / sy;
+                tn[i] = ScoreTau{0.5 * a0, 0.5 * a1, 0.5 * a2 + (r * r / (sy * sy) - 1.0) / sy, 0.0};
             }
             cur ^= 1;
             __syncthreads();
@@ -443,23 +450,24 @@ __global__ void __launch_bounds__(THREADS, 1) k_pf_score(const BatchedFilter *fi
                     const uint32_t b = run.sS[p], e = p + 1 < N ? run.sS[p + 1] : ne;
                     const uint32_t c = (anc[p] == p ? 1u : 0u) + (e - b);
                     rep[p] = c;
-                    W[p] = run.st.l[p] - log(static_cast<double>(c) + 1.0);
+                    xwn[p] = make_double2(xnow[p], run.st.l[p] - log(static_cast<double>(c) + 1.0));
                 }
             } else {
-                for (uint64_t p = threadIdx.x; p < N; p += THREADS) W[p] = run.st.l[p];
+                for (uint64_t p = threadIdx.x; p < N; p += THREADS) xwn[p] = make_double2(xnow[p], run.st.l[p]);
             }
             __syncthreads();
         }
         // the estimate: sum_i W_T^i tau_T^i / sum_i W_T^i, W_T the weights
         // of the last cloud (its log-weights relative to their maximum)
         double g0 = 0.0, g1 = 0.0, g2 = 0.0, gw = 0.0;
-        const double *tT = taub[cur];
+        const ScoreTau *tT = taub[cur];
         const double mT = run.st.lshift;
         for (uint64_t p = threadIdx.x; p < N; p += THREADS) {
             const double wp = exp(run.st.l[p] - mT);
-            g0 += wp * tT[p];
-            g1 += wp * tT[nm + p];
-            g2 += wp * tT[2 * nm + p];
+            const ScoreTau tp = tT[p];
+            g0 += wp * tp.a0;
+            g1 += wp * tp.a1;
+            g2 += wp * tp.a2;
             gw += wp;
         }
         g0 = block_sum(g0, shd);
@@ -1031,8 +1039,9 @@ int mckl_b200_batched_score(mckl_b200_batched_t *b, double *loglik, double *scor
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int ctas = std::max(1, std::min(b->F, sms));
     const uint64_t nm = b->nmax;
-    const size_t need = align256(ctas * 2 * nm * 8) + align256(ctas * nm * 8) + 2 * align256(ctas * nm * 4) +
-                        align256(ctas * 6 * nm * 8) + align256(static_cast<size_t>(b->F) * 24);
+    const size_t need = align256(ctas * nm * 8) + align256(ctas * 2 * nm * sizeof(double2)) +
+                        2 * align256(ctas * nm * 4) + align256(ctas * 2 * nm * sizeof(ScoreTau)) +
+                        align256(static_cast<size_t>(b->F) * 24);
     if (b->score_bytes < need) {
         if (b->score_mem) cudaFree(b->score_mem);
         b->score_mem = nullptr;
@@ -1051,11 +1060,11 @@ int mckl_b200_batched_score(mckl_b200_batched_t *b, double *loglik, double *scor
     };
     ScoreArgs A{};
     A.nmax = nm;
-    A.xb = reinterpret_cast<double *>(take(ctas * 2 * nm * 8));
-    A.w = reinterpret_cast<double *>(take(ctas * nm * 8));
+    A.xb = reinterpret_cast<double *>(take(ctas * nm * 8));
+    A.xw = reinterpret_cast<double2 *>(take(ctas * 2 * nm * sizeof(double2)));
     A.rep = reinterpret_cast<uint32_t *>(take(ctas * nm * 4));
     A.anc = reinterpret_cast<uint32_t *>(take(ctas * nm * 4));
-    A.tau = reinterpret_cast<double *>(take(ctas * 6 * nm * 8));
+    A.tau = reinterpret_cast<ScoreTau *>(take(ctas * 2 * nm * sizeof(ScoreTau)));
     A.score = reinterpret_cast<double *>(take(static_cast<size_t>(b->F) * 24));
     int rc = pf_score_launch(b->a, b->order, b->F, b->threads, b->queue, A, ctas, s);
     if (rc != MCKL_B200_OK) return rc;
