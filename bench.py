@@ -834,7 +834,7 @@ def cpu_smc_reference(w, T, nfilters=64):
     dt = time.perf_counter() - t0
     if rc != 0:
         raise RuntimeError("reference particle filter failed")
-    return dict(value=float(N.sum()) * T / dt, unit="particle-steps/s", cores=threads, kind="reference",
+    return dict(value=float(N.sum()) * T / dt, unit="particle-steps/s", cores=threads, kind="reference", seconds=dt,
                 sample=f"{len(idx)} of the {F} filters spread over the particle counts ({int(N.sum())} particles, "
                        f"T = {T}): MCKL SMCSampler + BackendSEQ per filter, OpenMP over filters; {dt:.1f} s")
 
@@ -869,7 +869,7 @@ def cpu_rng_reference(sample_log2=24):
                                    ctypes.c_void_p(out.ctypes.data), threads)
         total_bytes += n * bpv
         total_s += s
-    return dict(value=total_bytes / total_s / 1e9, unit="GB/s", cores=threads, kind="reference",
+    return dict(value=total_bytes / total_s / 1e9, unit="GB/s", cores=threads, kind="reference", seconds=total_s,
                 sample=f"every call of the workload at 2^{sample_log2} values (1/{1 << (LOG2N - sample_log2)} "
                        f"of the full size), OpenMP over block-aligned counter ranges")
 
@@ -922,7 +922,7 @@ def main():
             return
         if smc:
             w = reference_workload(F=args.filters, T=args.obs, seed=1234)
-        vals, base = [], None
+        vals, secs, base = [], [], None
         for i in range(args.warmup + args.steps):
             r = cpu_smc_reference(w, args.obs, 128) if smc else cpu_rng_reference()
             if r is None:
@@ -930,11 +930,14 @@ def main():
                 return
             if i >= args.warmup:
                 vals.append(r["value"])
+                secs.append(r["seconds"])
                 base = r
         v = statistics.median(vals)
         unit = "particle-steps/s" if smc else "GB/s"
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": unit, "n_gpus": args.gpus,
-                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.median(secs) * 1e3,
+                "step": "one bounded sample of the workload on the host cores (cpu_baseline.sample)",
+                "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64" if smc else "u32/f32/f64", "data": "synthetic",
                 "config": cfg, "cpu_baseline": strip(dict(base, value=v)),
                 "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
