@@ -367,6 +367,18 @@ __device__ __forceinline__ void st8(uint32_t *p, const uint32_t (&v)[8])
     reinterpret_cast<uint4 *>(p)[1] = make_uint4(v[4], v[5], v[6], v[7]);
 }
 
+__device__ __forceinline__ void st8(float *p, const float (&v)[8])
+{
+    reinterpret_cast<float4 *>(p)[0] = make_float4(v[0], v[1], v[2], v[3]);
+    reinterpret_cast<float4 *>(p)[1] = make_float4(v[4], v[5], v[6], v[7]);
+}
+
+__device__ __forceinline__ void st8(double *p, const double (&v)[8])
+{
+#pragma unroll
+    for (int q = 0; q < 4; ++q) reinterpret_cast<double2 *>(p)[q] = make_double2(v[2 * q], v[2 * q + 1]);
+}
+
 struct NoiseLayout {
     static constexpr uint64_t kUnits = 129;  // units per full chunk (the 32-bit division below uses 129)
     uint64_t N, m, tail, nu_tail, units, per_step;
@@ -595,8 +607,12 @@ struct FilterRun {
     // Step t: move, weight, normalise and (when ESS < N threshold) resample;
     // returns whether it resampled.  The resampling is in place (an empty
     // slot takes a copy of an occupied one, which is never overwritten); its
-    // placement stays in sS / ep[0, n_empty).
-    __device__ bool step(int t, double yt_d, double *shd, R *shr, unsigned long long *shu, uint32_t *shj)
+    // placement stays in sS / ep[0, n_empty).  With STAGEX the placement also
+    // stages each warp's parent positions in shx (THREADS / 32 x kWarpParents
+    // elements of shared memory), so a copy reads its source from there.
+    template <bool STAGEX = false>
+    __device__ bool step(int t, double yt_d, double *shd, R *shr, unsigned long long *shu, uint32_t *shj,
+        R *shx = nullptr)
     {
         const uint64_t N = lay.N;
         st.x = xc;
@@ -803,14 +819,28 @@ struct FilterRun {
                 const uint32_t P0 = b + warp * kWarpParents;
                 if (P0 >= N32) continue;  // warp-uniform; the loop holds no CTA barrier
                 const uint32_t q0 = P0 + lane * V;
-                uint32_t ss[V];
-                if (q0 + V <= N32) {
-                    ld8(sS + q0, ss);
-                } else {
+                // the warp's parents go to shared memory with their prefixes
+                // (STAGEX), read once and coalesced: a copy's source then
+                // costs no dependent global load behind the search (an empty
+                // slot staged here may be written meanwhile, but an empty
+                // slot is no parent)
+                R *wx = STAGEX ? shx + warp * kWarpParents : nullptr;
+                {
+                    uint32_t ss[V];
+                    R xv[V];
+                    if (q0 + V <= N32) {
+                        ld8(sS + q0, ss);
+                        if constexpr (STAGEX) ld8(xc + q0, xv);
+                    } else {
 #pragma unroll
-                    for (int k = 0; k < V; ++k) ss[k] = q0 + k < N32 ? sS[q0 + k] : ne;
+                        for (int k = 0; k < V; ++k) {
+                            ss[k] = q0 + k < N32 ? sS[q0 + k] : ne;
+                            if constexpr (STAGEX) xv[k] = q0 + k < N32 ? xc[q0 + k] : R(0);
+                        }
+                    }
+                    st8(wsw + lane * V, ss);
+                    if constexpr (STAGEX) st8(wx + lane * V, xv);
                 }
-                st8(wsw + lane * V, ss);
                 if (lane == 31) wsw[kWarpParents] = q0 + V < N32 ? sS[q0 + V] : ne;
                 __syncwarp();
                 const uint32_t A = wsw[0], B = wsw[kWarpParents];
@@ -824,13 +854,24 @@ struct FilterRun {
                 }
                 queued = __shfl_sync(0xffffffffu, queued, 0);
                 if (!queued) {
-                    for (uint32_t e = A + lane; e < B; e += 32) {
-                        uint32_t lo = 0;
+                    if constexpr (STAGEX) {
+                        for (uint32_t e = A + lane; e < B; e += 32) {
+                            uint32_t lo = 0;
 #pragma unroll
-                        for (uint32_t h = kWarpParents / 2; h >= 1; h >>= 1) lo += wsw[lo + h] <= e ? h : 0;
-                        const uint32_t slot = ep[e];
-                        xc[slot] = xc[P0 + lo];
-                        if constexpr (SHADOW) xsc[slot] = xsc[P0 + lo];
+                            for (uint32_t h = kWarpParents / 2; h >= 1; h >>= 1) lo += wsw[lo + h] <= e ? h : 0;
+                            const uint32_t slot = ep[e];
+                            xc[slot] = wx[lo];
+                            if constexpr (SHADOW) xsc[slot] = xsc[P0 + lo];
+                        }
+                    } else {
+                        for (uint32_t e = A + lane; e < B; e += 32) {
+                            uint32_t lo = 0;
+#pragma unroll
+                            for (uint32_t h = kWarpParents / 2; h >= 1; h >>= 1) lo += wsw[lo + h] <= e ? h : 0;
+                            const uint32_t slot = ep[e];
+                            xc[slot] = xc[P0 + lo];
+                            if constexpr (SHADOW) xsc[slot] = xsc[P0 + lo];
+                        }
                     }
                 }
                 __syncwarp();  // the staging area is rewritten by the next tile
@@ -876,6 +917,10 @@ __global__ void __launch_bounds__(THREADS, MINB) k_pf_batched(const BatchedFilte
     __shared__ R shr[33];
     __shared__ unsigned long long shu[33];
     __shared__ __align__(16) uint32_t shj[shj_words<THREADS>()];
+    // the placement's staged parent positions, where they fit beside shj in
+    // the 48 KB of static shared memory without cutting the residency
+    constexpr bool kStageX = THREADS <= 512 && sizeof(R) * (THREADS / 32) * kWarpParents <= 16384;
+    __shared__ __align__(16) R shx[kStageX ? (THREADS / 32) * kWarpParents : 1];
     __shared__ int sh_f;
     while (true) {
         if (threadIdx.x == 0) {
@@ -894,7 +939,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_pf_batched(const BatchedFilte
                 run.setup(filt[f], xa, xb, lw, scanS, epos, xsa, xsb, lws, threshold);
         }
         const double *yf = y + static_cast<uint64_t>(f) * (T + 1);
-        for (int t = 0; t <= T; ++t) run.step(t, yf[t], shd, shr, shu, shj);
+        for (int t = 0; t <= T; ++t) run.template step<kStageX>(t, yf[t], shd, shr, shu, shj, shx);
         if (threadIdx.x == 0) {
             loglik[f] = run.ll_sum;
             nresampled[f] = static_cast<uint32_t>(run.events);
