@@ -379,6 +379,13 @@ __device__ __forceinline__ void st8(double *p, const double (&v)[8])
     for (int q = 0; q < 4; ++q) reinterpret_cast<double2 *>(p)[q] = make_double2(v[2 * q], v[2 * q + 1]);
 }
 
+// A hint that the line holding p is read soon (prefetch.global.L1: nothing
+// waits on it and no register is held; p lies inside the buffer)
+__device__ __forceinline__ void prefetch_l1(const void *p)
+{
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 struct NoiseLayout {
     static constexpr uint64_t kUnits = 129;  // units per full chunk (the 32-bit division below uses 129)
     uint64_t N, m, tail, nu_tail, units, per_step;
@@ -623,6 +630,7 @@ struct FilterRun {
         Lse<R> acc;
         Lse<double> accs;
         // ---- noise, propagation, log-weights, online normaliser
+        const uint32_t fullu = static_cast<uint32_t>(lay.m * NoiseLayout::kUnits);  // units of whole chunks
         for (uint32_t u = threadIdx.x; u < static_cast<uint32_t>(lay.units); u += THREADS) {
             R v[8];
             double vs[8];
@@ -634,6 +642,19 @@ struct FilterRun {
             // generator keeps 16 loaded values live across it, which spills
             // at the 64-register budget of the resident shapes
             lay.slots(t, u, pa, pb, &lo, &hi, &src);
+            if (!st.init) {
+                // the particles of this thread's next unit, ahead of its loads
+                const uint32_t un = u + THREADS;
+                if (un < fullu) {
+                    const uint32_t c = un / 129u, pn = c * 1024u + 4u * (un - c * 129u);
+                    prefetch_l1(st.x + pn);
+                    prefetch_l1(st.x + pn + 512);
+                    if (!st.flat) {
+                        prefetch_l1(st.l + pn);
+                        prefetch_l1(st.l + pn + 512);
+                    }
+                }
+            }
             lay.words(gm, u, src, wr, wa);
             st.load4(pa, pb, lo, hi, old);
             st.move4(wr, wa, pa, pb, lo, hi, old, v, vs);
@@ -741,6 +762,7 @@ struct FilterRun {
         for (uint32_t b = 0; b < N32; b += TILE) {
             const uint32_t q0 = b + threadIdx.x * V;
             const bool whole = q0 + V <= N32;  // all V particles exist
+            if (q0 + TILE < N32) prefetch_l1(st.l + q0 + TILE);  // this thread's next tile
             R lv[V];
             if (whole) {
                 ld8(st.l + q0, lv);
@@ -819,6 +841,10 @@ struct FilterRun {
                 const uint32_t P0 = b + warp * kWarpParents;
                 if (P0 >= N32) continue;  // warp-uniform; the loop holds no CTA barrier
                 const uint32_t q0 = P0 + lane * V;
+                if (q0 + TILE < N32) {  // the warp's next tile
+                    prefetch_l1(sS + q0 + TILE);
+                    if constexpr (STAGEX) prefetch_l1(xc + q0 + TILE);
+                }
                 // the warp's parents go to shared memory with their prefixes
                 // (STAGEX), read once and coalesced: a copy's source then
                 // costs no dependent global load behind the search (an empty
