@@ -762,7 +762,6 @@ struct FilterRun {
         for (uint32_t b = 0; b < N32; b += TILE) {
             const uint32_t q0 = b + threadIdx.x * V;
             const bool whole = q0 + V <= N32;  // all V particles exist
-            if (q0 + TILE < N32) prefetch_l1(st.l + q0 + TILE);  // this thread's next tile
             R lv[V];
             if (whole) {
                 ld8(st.l + q0, lv);
@@ -841,10 +840,6 @@ struct FilterRun {
                 const uint32_t P0 = b + warp * kWarpParents;
                 if (P0 >= N32) continue;  // warp-uniform; the loop holds no CTA barrier
                 const uint32_t q0 = P0 + lane * V;
-                if (q0 + TILE < N32) {  // the warp's next tile
-                    prefetch_l1(sS + q0 + TILE);
-                    if constexpr (STAGEX) prefetch_l1(xc + q0 + TILE);
-                }
                 // the warp's parents go to shared memory with their prefixes
                 // (STAGEX), read once and coalesced: a copy's source then
                 // costs no dependent global load behind the search (an empty
