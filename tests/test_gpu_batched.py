@@ -64,6 +64,33 @@ def test_batched_fp64_matches_plain(env, small, threads):
     assert close >= len(ll) - 2
 
 
+def test_batched_fp64_matches_oracle(env, small):
+    """The FP64 batched filters directly against the oracle's particle filter
+    in the reference's step order (algorithm/smc.hpp:389-406: move, weight,
+    ESS, systematic resampling at ESS < N/2), filter by filter: the same
+    number of resampling events everywhere, log-likelihoods within 1e-9
+    relative except where a uniform within a few ULPs of a cumulative weight
+    flipped an ancestor (at most two of the 48 filters, and then within the
+    Monte Carlo noise of one ancestor, 1e-4)."""
+    mb, orc = env
+    w = small
+    b = mb.BatchedFilters(w["N"], w["y"], w["phi"], w["sx"], w["sy"], w["mkeys"], w["rkeys"], fp64=True)
+    b.config(threads=256, ctas_per_sm=4)
+    b.run()
+    ll, nr = b.results()
+    b.close()
+    close = 0
+    for f in range(len(ll)):
+        r = orc.pf_ar1(int(w["N"][f]), w["y"][f], w["phi"][f], w["sx"][f], w["sy"][f], w["sd0"][f],
+                       tuple(w["mkeys"][f]), tuple(w["rkeys"][f]), record=False)
+        assert int(nr[f]) == int(r["resampled"].sum()), f
+        if abs(ll[f] - r["loglik"]) <= 1e-9 * abs(r["loglik"]):
+            close += 1
+        else:
+            assert abs(ll[f] - r["loglik"]) <= 1e-4 * abs(r["loglik"]), (f, ll[f], r["loglik"])
+    assert close >= len(ll) - 2
+
+
 def test_batched_fp32_accuracy_and_graph(env, small):
     mb, orc = env
     w = small
