@@ -1,7 +1,8 @@
 """Benchmark of the B200 path (one JSON line on rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mckl_b200|reference]
-                    [--workload smc|rng] [--filters F] [--obs T] [--parts all|timed]
+                    [--workload smc|rng|callers|plain|adjoint] [--filters F] [--obs T] [--parts all|timed]
+                    [--sets S] [--particles N]
 
 Workload `smc` (default, the batched SMC configuration): F = 4096 independent
 AR(1) bootstrap filters, phi ~ U[0.5, 0.99], sx ~ U[0.5, 2], sy ~ U[0.2, 1] and
@@ -885,9 +886,13 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mckl_b200", choices=["mckl_b200", "reference"])
-    ap.add_argument("--workload", default="smc", choices=["smc", "rng", "callers", "plain"],
+    ap.add_argument("--workload", default="smc", choices=["smc", "rng", "callers", "plain", "adjoint"],
                     help="callers: only the index matrix / weighted estimate / PMCMC measurements; plain: only the "
-                         "plain FP64 filter at N = 2^20 (T = --obs, 1000 by default); one JSON object each")
+                         "plain FP64 filter at N = 2^20 (T = --obs, 1000 by default); adjoint: only the "
+                         "differentiated configuration (--sets parameter sets x --particles x T = --obs, 1000 by "
+                         "default); one JSON object each")
+    ap.add_argument("--sets", type=int, default=256, help="parameter sets of the adjoint workload")
+    ap.add_argument("--particles", type=int, default=1 << 16, help="particles per set of the adjoint workload")
     ap.add_argument("--filters", type=int, default=4096)
     ap.add_argument("--obs", type=int, default=500)
     ap.add_argument("--parts", default="all", choices=["all", "timed"])
@@ -957,6 +962,14 @@ def main():
             c3 = bench_plain_c3(T=T)
             c3.pop("y")
             print(json.dumps({"workload": "plain", "n_gpus": 1, "plain_c3": c3}))
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+    if args.workload == "adjoint":
+        if rank == 0:
+            T = args.obs if args.obs != 500 else 1000
+            adj = bench_adjoint(rank, dev, sets=args.sets, N=args.particles, T=T)
+            print(json.dumps({"workload": "adjoint", "n_gpus": 1, "adjoint": adj}))
         if world > 1:
             torch.distributed.destroy_process_group()
         return
