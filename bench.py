@@ -79,8 +79,8 @@ MUFU_PER_CLK_SM = 16
 # From the ncu capture summarised in profiles/k_pf_batched_c4.md: warp
 # instructions per particle-step of the batched kernel, and DRAM bytes per
 # particle-step (read + write), measured on a 2.4e8 particle-step case.
-WARP_INSTR_PER_PS = 8.83
-DRAM_BYTES_PER_PS = 13.7
+WARP_INSTR_PER_PS = 8.47
+DRAM_BYTES_PER_PS = 13.75
 
 
 def measured_peaks():
