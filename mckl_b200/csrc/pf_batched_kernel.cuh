@@ -56,6 +56,9 @@ struct Math<float> {
     __device__ static float radius(float u) { return sqrtf(-2.0f * logf(u)); }
     __device__ static void sincos2pi(float v, float *s, float *c) { sincospif(2.0f * v, s, c); }
     __device__ static float cos2pi(float v) { return cospif(2.0f * v); }
+    // exp2 of the scaled argument (its rounding adds at most 2^-20 relative
+    // for the arguments the weights take, |a| <= 20 where it matters): the
+    // normaliser's terms and the fixed-point weights, summed in FP64
     __device__ static float exp(float a) { return exp2f(__fmul_rn(a, 1.44269504088896341f)); }
     __device__ static float mul(float a, float b) { return __fmul_rn(a, b); }
     __device__ static float add(float a, float b) { return __fadd_rn(a, b); }
