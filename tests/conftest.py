@@ -11,7 +11,7 @@ by the driver and by torch, which would turn a device that is merely slow to
 come up into a whole session without CUDA.
 
 * When the ``gpu`` marker was asked for explicitly (``-m gpu``) the probe is
-  retried for up to ``MCKL_B200_GPU_PROBE_S`` seconds (default 60) and, if the
+  retried for up to ``MCKL_B200_GPU_PROBE_S`` seconds (default 120) and, if the
   device never answers, the session FAILS with the driver's return code and
   the environment it saw.  A GPU run never passes by skipping its tests.
 * Otherwise (a plain ``pytest tests/`` on a CPU-only host) the GPU tests are
@@ -88,7 +88,7 @@ def probe_gpu(config):
     if _STATE["ok"] is not None:
         return _STATE["ok"]
     explicit = _gpu_explicitly_selected(config)
-    limit = float(os.environ.get("MCKL_B200_GPU_PROBE_S", "60")) if explicit else 0.0
+    limit = float(os.environ.get("MCKL_B200_GPU_PROBE_S", "120")) if explicit else 0.0
     t0 = time.monotonic()
     attempts = 0
     while True:
